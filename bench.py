@@ -1,0 +1,405 @@
+"""Benchmark of the single-pass replace kernel on the 2 GiB / 1 GiB single-pair workload.
+
+Workload (one "step"): three single-pair replaces, each one launch of the sm_100a kernel:
+  (i)   2 GiB of b"a", b"aa" -> b"X"            (maximal self-overlap, 2**30 matches, shrink)
+  (ii)  2 GiB of b"a", b"a" -> b"bcd"           (6 GiB output, 64-bit offsets, expand)
+  (iii) 1 GiB i.i.d. uniform bytes, b"\\x00\\x00\\x01" -> b""  (embedded NULs, deletion)
+Metric: GB/s of (input + output) bytes, 1 GB = 1e9 bytes.
+
+value:  device-resident inputs (HBM), K steps timed with CUDA events on the launching
+        stream; every input is larger than the 126 MB L2, so no flush is needed.
+e2e:    the same step through the reference-facing C ABI call cuda_replace_unified with
+        page-locked host inputs: H2D, kernel, D2H of the result inside the timed region.
+cpu_baseline: CPython bytes.replace (single thread) on a bounded sample of the same cases.
+--impl reference: the reference's CPU path (bytes.replace) alone, on all three cases.
+
+Multi-GPU: the path does not shard across GPUs here (replicas only): under torchrun each
+rank runs the same step on its own GPU, time = max over ranks, value = sum of bytes.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+GiB = 1 << 30
+MiB = 1 << 20
+SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+CASES = [("a-run aa->X", b"aa", b"X"), ("a-run a->bcd", b"a", b"bcd"), ("random 00 00 01->''", b"\x00\x00\x01", b"")]
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=float, default=1.0, help="input size multiplier (1.0 = full size)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ------------------------------------------------------------------ distributed plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend: str):
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float, device=None) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float, device=None) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def aggregate_replicas(bytes_per_rank: float, secs_per_rank: float, dist: Dist, device=None):
+    """Replicas: total bytes over all ranks divided by the slowest rank's time."""
+    total = dist.sum(bytes_per_rank, device)
+    slowest = dist.max(secs_per_rank, device)
+    return total, slowest
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={SMI_FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ inputs
+def make_inputs(scale: float):
+    import numpy as np
+
+    from cuda_replace_b200 import workloads as WL
+    n_run = int(2 * GiB * scale) // 16 * 16
+    n_rand = int(1 * GiB * scale) // 16 * 16
+    rand = np.random.default_rng(2).integers(0, 256, size=n_rand, dtype=np.uint8)
+    return n_run, n_rand, rand, WL
+
+
+def expected_lengths(n_run: int, rand_bytes: bytes):
+    from oracle import oracle as O  # checker only
+    n3, k3, _ = O.replace_len(rand_bytes, b"\x00\x00\x01", 0)
+    return [(n_run // 2 + n_run % 2, n_run // 2), (3 * n_run, n_run), (n3, k3)]
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    p = REPO / "profiles" / "replace_tiles_c2_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except json.JSONDecodeError:
+            return None
+    return None
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_sample(rand_np, budget_scale: float = 1.0):
+    """bytes.replace on a bounded sample of the three cases; returns (bytes, seconds, desc)."""
+    sizes = [int(512 * MiB * budget_scale), int(256 * MiB * budget_scale), min(len(rand_np), int(GiB * budget_scale))]
+    total_b, total_t = 0, 0.0
+    srcs = [b"a" * sizes[0], b"a" * sizes[1], rand_np[:sizes[2]].tobytes()]
+    for (name, pat, rep), src in zip(CASES, srcs):
+        t0 = time.perf_counter()
+        out = src.replace(pat, rep)
+        dt = time.perf_counter() - t0
+        total_b += len(src) + len(out)
+        total_t += dt
+        del out
+    desc = (f"CPython bytes.replace, 1 thread: {sizes[0] >> 20} MiB a-run aa->X, {sizes[1] >> 20} MiB a-run a->bcd, "
+            f"{sizes[2] >> 20} MiB random 00 00 01->'' (same generators as the GPU step)")
+    return total_b, total_t, desc
+
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return 0
+    import numpy as np
+    rand = np.random.default_rng(2).integers(0, 256, size=int(GiB * min(args.scale, 1.0)), dtype=np.uint8)
+    scale = 0.25 * min(args.scale, 1.0)
+    for _ in range(args.warmup):
+        cpu_sample(rand, scale)
+    tb, tt = 0, 0.0
+    desc = ""
+    for _ in range(args.steps):
+        b, t, desc = cpu_sample(rand, scale)
+        tb += b
+        tt += t
+    value = tb / tt / 1e9
+    line = {
+        "impl": "reference", "metric": "GB/s (in+out), single-pair replace", "value": round(value, 4),
+        "unit": "GB/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tt / args.steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+        "config": {"workload": "2 GiB a-run aa->X + 2 GiB a-run a->bcd + 1 GiB random 00 00 01->'' "
+                               "(each step a 1/4-size sample on the CPU)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": 1, "kind": "port",
+                         "sample": desc + "; the reference's own CPU path (test/test.py:102-112)"},
+        "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ main arm
+def run_ours(args, dist: Dist):
+    import numpy as np
+    import torch
+
+    from cuda_replace_b200 import build as B
+    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib, Session
+
+    torch.cuda.set_device(dist.local_rank)
+    dev = torch.device("cuda", dist.local_rank)
+    dist.init("nccl")
+    lib = CudaReplaceLib(str(B.LIB_PATH))
+    n_run, n_rand, rand_np, _ = make_inputs(args.scale)
+
+    # device-resident inputs and outputs (pad 64 B: the kernel reads up to n rounded to 16)
+    d_run = torch.full((n_run + 64,), ord("a"), dtype=torch.uint8, device=dev)
+    d_rand = torch.empty(n_rand + 64, dtype=torch.uint8, device=dev)
+    d_rand[:n_rand].copy_(torch.from_numpy(rand_np))
+    outs = [torch.empty(n_run + 64, dtype=torch.uint8, device=dev),
+            torch.empty(3 * n_run + 64, dtype=torch.uint8, device=dev),
+            torch.empty(n_rand + 64, dtype=torch.uint8, device=dev)]
+    caps = [n_run, 3 * n_run, n_rand]
+    ins = [(d_run, n_run), (d_run, n_run), (d_rand, n_rand)]
+    stream = torch.cuda.Stream(device=dev)
+    sessions = [Session(lib, b"") for _ in CASES]
+
+    exp = expected_lengths(n_run, rand_np.tobytes()) if dist.rank == 0 else None
+
+    def one_step(events=None):
+        for i, ((name, pat, rep), (d_in, n), out, cap, s) in enumerate(zip(CASES, ins, outs, caps, sessions)):
+            if events is not None:
+                events[i][0].record(stream)
+            s.apply_device_async(d_in.data_ptr(), n, pat, rep, out.data_ptr(), cap, stream.cuda_stream)
+            if events is not None:
+                events[i][1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 0)):
+            one_step()
+    torch.cuda.synchronize()
+    # correctness of the warm-up outputs (lengths + kept counts) against the oracle
+    results = [s.device_result() for s in sessions]
+    if exp is not None:
+        for (name, _, _), got, want in zip(CASES, results, exp):
+            if tuple(got) != tuple(want):
+                raise SystemExit(f"bench self-check failed for {name}: got {got}, want {want}")
+    bytes_per_step = sum(n + r[0] for (_, n), r in zip(ins, results))
+    launches0 = sum(s.stats()[1] for s in sessions)
+
+    per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in CASES] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(dist.local_rank)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    start.record(stream)
+    for k in range(args.steps):
+        one_step(per_launch[k])
+    end.record(stream)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    dist.barrier()
+    secs = start.elapsed_time(end) / 1e3
+    gpu_launches = sum(s.stats()[1] for s in sessions) - launches0
+    total_bytes, slowest = aggregate_replicas(bytes_per_step * args.steps, secs, dist, dev)
+    value = total_bytes / slowest / 1e9
+
+    # roofline of the replace kernel: algorithmic (in+out) bytes / mean launch duration
+    launch_ms = [[per_launch[k][i][0].elapsed_time(per_launch[k][i][1]) for k in range(args.steps)]
+                 for i in range(len(CASES))]
+    case_bytes = [n + r[0] for (_, n), r in zip(ins, results)]
+    achieved = sum(case_bytes) / (sum(statistics.mean(m) for m in launch_ms) / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic()
+
+    # e2e through the reference-facing C ABI with page-locked host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, lib, n_run, rand_np, dist, dev)
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+        cb, ct, desc = cpu_sample(rand_np, min(args.scale, 1.0))
+        cpu = {"value": round(cb / ct / 1e9, 4), "unit": "GB/s", "cores": 1, "kind": "port", "sample": desc}
+
+    for s in sessions:
+        s.close()
+    if dist.rank == 0:
+        line = {
+            "metric": "GB/s (in+out), single-pair replace", "value": round(value, 2), "unit": "GB/s",
+            "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(slowest / args.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+            "config": {
+                "workload": (f"{n_run / GiB:g} GiB a-run aa->X + {n_run / GiB:g} GiB a-run a->bcd + "
+                             f"{n_rand / GiB:g} GiB random 00 00 01->'' (one launch each)"),
+                "bytes_in_plus_out_per_step": bytes_per_step, "l2": "inputs larger than L2 (126 MB), no flush",
+                "parallelism": f"replicas x{dist.world}",
+                "per_case_gbs": {c[0]: round(b / (statistics.mean(m) / 1e3) / 1e9, 1)
+                                 for c, b, m in zip(CASES, case_bytes, launch_ms)},
+            },
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "traffic": traffic.get("bytes_per_step") if traffic else None,
+                         "algorithmic_bytes": sum(case_bytes)},
+            "gpu_launches": gpu_launches,
+            "clocks": clock_info,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    del outs, d_run, d_rand
+    dist.close()
+    return 0
+
+
+def run_e2e(args, lib, n_run, rand_np, dist: Dist, dev):
+    import torch
+    h_run = torch.full((n_run,), ord("a"), dtype=torch.uint8).pin_memory()
+    h_rand = torch.from_numpy(rand_np).pin_memory()
+    srcs = [(h_run, n_run), (h_run, n_run), (h_rand, len(rand_np))]
+    out_ptr = C.POINTER(C.c_uint8)()
+    out_len = C.c_size_t()
+    pats = [(C.create_string_buffer(p, len(p) or 1), len(p), C.create_string_buffer(r, len(r) or 1), len(r))
+            for _, p, r in CASES]
+
+    def step():
+        h2d = d2h = 0
+        for (h, n), (pb, pl, rb, rl) in zip(srcs, pats):
+            rc = lib.lib.cuda_replace_unified(C.cast(h.data_ptr(), C.POINTER(C.c_uint8)), n,
+                                              C.cast(pb, C.POINTER(C.c_uint8)), pl,
+                                              C.cast(rb, C.POINTER(C.c_uint8)), rl, C.byref(out_ptr), C.byref(out_len))
+            if rc != 0:
+                raise RuntimeError(f"cuda_replace_unified rc={rc}")
+            h2d += n
+            d2h += out_len.value
+            lib.lib.cuda_free_host(out_ptr)
+        return h2d, d2h
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    steps = max(1, min(args.steps, 5))
+    dist.barrier()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(steps):
+        a, b = step()
+        h2d += a
+        d2h += b
+    secs = time.perf_counter() - t0
+    total, slowest = aggregate_replicas(h2d + d2h, secs, dist, dev)
+    return {"value": round(total / slowest / 1e9, 3), "unit": "GB/s",
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
+            "steps": steps, "api": "cuda_replace_unified (page-locked host input)"}
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    dist = Dist()
+    if args.impl == "reference":
+        return run_reference(args, dist)
+    return run_ours(args, dist)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

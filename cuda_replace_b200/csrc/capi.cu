@@ -1,0 +1,727 @@
+// capi.cu - sessions, memory management and the C ABI of libcuda_replace.so.
+//
+// Mirrors the exports of RAZZULLIX/cuda_replace (cuda_replace.cu:2164-2603): same names,
+// signatures, ownership rules and return codes (see include/cuda_replace.h). The session
+// keeps two device buffers that swap roles after every apply (input -> output), a small
+// look-back scratch area (per-tile status, function tables, inclusive prefixes) that
+// grows with the input, and a device result block read back once per apply.
+//
+// Differences from the reference that callers can observe, all towards bytes.replace:
+//  * An empty pattern inserts the replacement before every byte and at the end, as
+//    bytes.replace does; the reference leaves the buffer unchanged (cuda_replace.cu:2104).
+//  * apply_seeded honours negative carry-ins (the reference's default fused path ignores
+//    them, cuda_replace.cu:859) and reports the real last kept start.
+//  * Positions, counts and offsets are 64-bit end to end (the reference truncates to int
+//    at cuda_replace.cu:159-160, 609, 668, 1418).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <unordered_map>
+#include <vector>
+
+#include "cuda_replace.h"
+#include "replace_kernels.h"
+
+#define CR_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+using crb::ApplyResult;
+using crb::ReplaceParams;
+using crb::TileIncl;
+
+constexpr int kErrUnknown = 999;  // cudaErrorUnknown
+constexpr size_t kAllocQuantum = 2ull << 20;
+
+size_t round_up(size_t x, size_t q) { return (x + q - 1) / q * q; }
+
+// ------------------------------------------------------------------ page-locked host pool
+// Results are handed to the caller in page-locked memory that it frees with cuda_free_host.
+// Pinning fresh memory for every result costs far more than the copy itself, so freed
+// blocks are kept (up to kMaxIdle bytes) and reused for later results of similar size.
+class PinnedPool {
+ public:
+  void* get(size_t n, cudaError_t* err) {
+    const size_t want = round_up(n ? n : 1, 64 << 10);
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      auto it = idle_.lower_bound(want);
+      if (it != idle_.end() && it->first <= want + want / 2 + (64ull << 20)) {
+        void* p = it->second;
+        idle_bytes_ -= it->first;
+        idle_.erase(it);
+        *err = cudaSuccess;
+        return p;
+      }
+    }
+    void* p = nullptr;
+    *err = cudaMallocHost(&p, want);
+    if (*err != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> g(mu_);
+    sizes_[p] = want;
+    return p;
+  }
+  void put(void* p) {
+    if (!p) return;
+    std::vector<void*> evict;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      auto s = sizes_.find(p);
+      if (s == sizes_.end()) {
+        evict.push_back(p);  // not ours: release directly
+      } else {
+        idle_.emplace(s->second, p);
+        idle_bytes_ += s->second;
+        while (idle_bytes_ > kMaxIdle && !idle_.empty()) {
+          auto big = std::prev(idle_.end());
+          idle_bytes_ -= big->first;
+          sizes_.erase(big->second);
+          evict.push_back(big->second);
+          idle_.erase(big);
+        }
+      }
+    }
+    for (void* q : evict) cudaFreeHost(q);
+  }
+
+ private:
+  static constexpr size_t kMaxIdle = 24ull << 30;
+  std::mutex mu_;
+  std::multimap<size_t, void*> idle_;
+  std::unordered_map<void*, size_t> sizes_;
+  size_t idle_bytes_ = 0;
+};
+
+PinnedPool& pinned_pool() {
+  static PinnedPool* pool = new PinnedPool();  // never destroyed: CUDA may be torn down first at exit
+  return *pool;
+}
+
+// ------------------------------------------------------------------ session
+struct Session {
+  std::mutex mtx;
+  bool alive = true;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+
+  uint8_t* buf = nullptr;  // current contents (len bytes)
+  size_t buf_cap = 0;
+  uint8_t* alt = nullptr;  // output of the next apply; holds the previous input afterwards
+  size_t alt_cap = 0;
+  size_t len = 0;
+
+  uint32_t* status = nullptr;  // look-back scratch
+  TileIncl* incl = nullptr;
+  size_t tiles_cap = 0;
+  unsigned long long* agg = nullptr;
+  size_t agg_cap = 0;
+  ApplyResult* res = nullptr;       // device
+  ApplyResult* res_host = nullptr;  // page-locked mirror
+  uint8_t* ext = nullptr;           // device copy of long patterns / replacements
+  size_t ext_cap = 0;
+  uint8_t* ext_host = nullptr;
+  size_t ext_host_cap = 0;
+
+  uint32_t epoch = 0;
+  unsigned long long launches = 0;
+  unsigned long long kept_last = 0;
+
+  cudaStream_t async_stream = nullptr;  // stream of the last cuda_replace_apply_device_async
+  uint32_t async_epoch = 0;
+
+  // the most recent apply, for query_prefix: 0 none, 1 no match possible, 2 kernel, 3 empty pattern
+  int q_kind = 0;
+  unsigned long long q_n = 0;
+  ReplaceParams q_params;
+};
+
+cudaError_t dev_grow(uint8_t** ptr, size_t* cap, size_t need, bool keep, size_t keep_len, cudaStream_t st) {
+  if (*cap >= need && *ptr) return cudaSuccess;
+  const size_t new_cap = round_up(need + need / 8 + 4096, kAllocQuantum);
+  uint8_t* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, new_cap);
+  if (e != cudaSuccess) {
+    // retry without headroom before giving up
+    const size_t tight = round_up(need + 4096, 4096);
+    e = cudaMalloc(&p, tight);
+    if (e != cudaSuccess) return e;
+    *cap = tight;
+  } else {
+    *cap = new_cap;
+  }
+  if (keep && *ptr && keep_len) {
+    e = cudaMemcpyAsync(p, *ptr, keep_len, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      cudaFree(p);
+      return e;
+    }
+  }
+  if (*ptr) cudaFree(*ptr);
+  *ptr = p;
+  return cudaSuccess;
+}
+
+cudaError_t ensure_scratch(Session* s, size_t tiles, size_t entries_per_tile) {
+  if (tiles > s->tiles_cap) {
+    const size_t cap = tiles + tiles / 8 + 64;
+    uint32_t* st = nullptr;
+    TileIncl* in = nullptr;
+    cudaError_t e = cudaMalloc(&st, cap * sizeof(uint32_t));
+    if (e != cudaSuccess) return e;
+    e = cudaMalloc(&in, cap * sizeof(TileIncl));
+    if (e != cudaSuccess) {
+      cudaFree(st);
+      return e;
+    }
+    e = cudaMemsetAsync(st, 0, cap * sizeof(uint32_t), s->stream);
+    if (e != cudaSuccess) {
+      cudaFree(st);
+      cudaFree(in);
+      return e;
+    }
+    if (s->status) cudaFree(s->status);
+    if (s->incl) cudaFree(s->incl);
+    s->status = st;
+    s->incl = in;
+    s->tiles_cap = cap;
+  }
+  const size_t entries = tiles * entries_per_tile;
+  if (entries > s->agg_cap) {
+    const size_t cap = entries + entries / 8 + 1024;
+    unsigned long long* a = nullptr;
+    cudaError_t e = cudaMalloc(&a, cap * sizeof(unsigned long long));
+    if (e != cudaSuccess) return e;
+    if (s->agg) cudaFree(s->agg);
+    s->agg = a;
+    s->agg_cap = cap;
+  }
+  return cudaSuccess;
+}
+
+uint32_t next_epoch(Session* s) {
+  if (s->epoch >= (1u << 30) - 2) {
+    // wrap: clear every status word so old epochs cannot alias new ones
+    cudaMemsetAsync(s->status, 0, s->tiles_cap * sizeof(uint32_t), s->stream);
+    s->epoch = 0;
+  }
+  return ++s->epoch;
+}
+
+void session_free(Session* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->buf) cudaFree(s->buf);
+  if (s->alt) cudaFree(s->alt);
+  if (s->status) cudaFree(s->status);
+  if (s->incl) cudaFree(s->incl);
+  if (s->agg) cudaFree(s->agg);
+  if (s->res) cudaFree(s->res);
+  if (s->res_host) cudaFreeHost(s->res_host);
+  if (s->ext) cudaFree(s->ext);
+  if (s->ext_host) cudaFreeHost(s->ext_host);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+int session_create(Session** out) {
+  *out = nullptr;
+  Session* s = new (std::nothrow) Session();
+  if (!s) return -2;
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&s->res, sizeof(ApplyResult));
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->res, 0, sizeof(ApplyResult), s->stream);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->res_host, sizeof(ApplyResult));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) {
+    session_free(s);
+    return (int)e;
+  }
+  *out = s;
+  return 0;
+}
+
+// Upload src[0, len) into the session buffer.
+int session_load(Session* s, const uint8_t* src, size_t len) {
+  if (len && !src) return -1;
+  cudaError_t e = dev_grow(&s->buf, &s->buf_cap, len ? len : 1, false, 0, s->stream);
+  if (e != cudaSuccess) return (int)e;
+  if (len) {
+    e = cudaMemcpyAsync(s->buf, src, len, cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return (int)e;
+  }
+  e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return (int)e;
+  s->len = len;
+  s->q_kind = 0;
+  return 0;
+}
+
+// Copy host bytes that do not fit in the launch parameters to the device.
+cudaError_t upload_ext(Session* s, const uint8_t* pat, uint32_t L, const uint8_t* rep, uint32_t R) {
+  const size_t need = round_up(L, 16) + round_up(R, 16) + 32;
+  if (need > s->ext_host_cap) {
+    if (s->ext_host) {
+      cudaStreamSynchronize(s->stream);
+      cudaFreeHost(s->ext_host);
+      s->ext_host = nullptr;
+    }
+    cudaError_t e = cudaMallocHost(&s->ext_host, need);
+    if (e != cudaSuccess) return e;
+    s->ext_host_cap = need;
+  }
+  if (need > s->ext_cap) {
+    cudaStreamSynchronize(s->stream);
+    if (s->ext) cudaFree(s->ext);
+    s->ext = nullptr;
+    cudaError_t e = cudaMalloc(&s->ext, need);
+    if (e != cudaSuccess) return e;
+    s->ext_cap = need;
+  }
+  cudaError_t e = cudaStreamSynchronize(s->stream);  // staging may still feed an earlier copy
+  if (e != cudaSuccess) return e;
+  if (L) memcpy(s->ext_host, pat, L);
+  if (R) memcpy(s->ext_host + round_up(L, 16), rep, R);
+  return cudaMemcpyAsync(s->ext, s->ext_host, need, cudaMemcpyHostToDevice, s->stream);
+}
+
+// Worst-case output length of one apply, saturating at SIZE_MAX.
+size_t output_bound(size_t n, uint32_t L, uint32_t R) {
+  if (L == 0) {
+    const unsigned __int128 b = (unsigned __int128)n * (R + 1ull) + R;
+    return b > (unsigned __int128)SIZE_MAX ? SIZE_MAX : (size_t)b;
+  }
+  if (R <= L) return n;
+  const unsigned __int128 b = (unsigned __int128)n + (unsigned __int128)(n / L) * (R - L);
+  return b > (unsigned __int128)SIZE_MAX ? SIZE_MAX : (size_t)b;
+}
+
+void swap_buffers(Session* s) {
+  std::swap(s->buf, s->alt);
+  std::swap(s->buf_cap, s->alt_cap);
+}
+
+// One apply. block_before: candidates starting before it are not taken.
+int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, int rep_len,
+              unsigned long long block_before, long long* out_last, size_t* new_len) {
+  if (pat_len < 0 || rep_len < 0) return -1;
+  if ((pat_len > 0 && !pat) || (rep_len > 0 && !rep)) return -1;
+  const uint32_t L = (uint32_t)pat_len, R = (uint32_t)rep_len;
+  if (L > crb::kMaxLen || R > crb::kMaxLen) return -4;
+  const size_t n = s->len;
+  cudaError_t e;
+
+  if (L == 0) {  // bytes.replace(b"", rep)
+    const size_t out_n = output_bound(n, 0, R);
+    if (out_n == SIZE_MAX) return (int)cudaErrorMemoryAllocation;
+    e = dev_grow(&s->alt, &s->alt_cap, out_n ? out_n : 1, false, 0, s->stream);
+    if (e != cudaSuccess) return (int)e;
+    if (R) {
+      e = upload_ext(s, nullptr, 0, rep, R);
+      if (e != cudaSuccess) return (int)e;
+    }
+    if (out_n) {
+      e = crb::launch_empty_pattern(s->buf, n, s->ext, R, s->alt, s->stream);
+      if (e != cudaSuccess) return (int)e;
+      ++s->launches;
+    }
+    e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return (int)e;
+    swap_buffers(s);
+    s->len = out_n;
+    s->q_kind = 3;
+    s->q_n = n;
+    s->kept_last = n + 1;
+    if (out_last) *out_last = (long long)n;
+    if (new_len) *new_len = out_n;
+    return 0;
+  }
+
+  if (n < L) {  // no occurrence possible: the buffer is unchanged
+    s->q_kind = 1;
+    s->q_n = n;
+    s->kept_last = 0;
+    if (out_last) *out_last = -1;
+    if (new_len) *new_len = n;
+    return 0;
+  }
+
+  ReplaceParams p;
+  memset(&p, 0, sizeof(p));
+  crb::prepare_pattern_fields(p, pat, L);
+  p.R = R;
+  const size_t tiles = (n + crb::kTile - 1) / crb::kTile;
+  if (tiles > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;
+  p.num_tiles = (uint32_t)tiles;
+  e = ensure_scratch(s, tiles, p.agg_entries);
+  if (e != cudaSuccess) return (int)e;
+
+  const size_t bound = output_bound(n, L, R);
+  size_t want = bound;
+  const size_t generous = std::max<size_t>(4 * n, n + (256ull << 20));
+  if (bound > generous) want = std::max<size_t>(s->alt_cap, std::min<size_t>(bound, 2 * n + (64ull << 20)));
+  e = dev_grow(&s->alt, &s->alt_cap, want ? want : 1, false, 0, s->stream);
+  if (e != cudaSuccess) return (int)e;
+
+  if (L > (uint32_t)crb::kInlineMax || R > (uint32_t)crb::kInlineMax) {
+    e = upload_ext(s, pat, L, rep, R);
+    if (e != cudaSuccess) return (int)e;
+    p.pat_ext = s->ext;
+    p.rep_ext = s->ext + round_up(L, 16);
+  }
+  if (L <= (uint32_t)crb::kInlineMax) memcpy(p.pat, pat, L);
+  if (R <= (uint32_t)crb::kInlineMax && R) memcpy(p.rep, rep, R);
+  p.in = s->buf;
+  p.n = n;
+  p.block_before = block_before;
+  p.status = s->status;
+  p.incl = s->incl;
+  p.agg = s->agg;
+  p.res = s->res;
+
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    p.out = s->alt;
+    p.out_cap = s->alt_cap;
+    p.epoch = next_epoch(s);
+    e = crb::launch_replace(p, s->stream, nullptr);
+    if (e != cudaSuccess) return (int)e;
+    ++s->launches;
+    e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return (int)e;
+    const ApplyResult r = *s->res_host;
+    if (r.error_epoch == p.epoch) return kErrUnknown;
+    if (r.overflow_epoch == p.epoch) {
+      if (attempt == 1) return kErrUnknown;
+      e = dev_grow(&s->alt, &s->alt_cap, r.out_len, false, 0, s->stream);
+      if (e != cudaSuccess) return (int)e;
+      continue;
+    }
+    swap_buffers(s);
+    s->len = (size_t)r.out_len;
+    s->q_kind = 2;
+    s->q_n = n;
+    s->q_params = p;
+    s->kept_last = r.kept;
+    if (out_last) *out_last = r.kept ? r.last_kept : -1;
+    if (new_len) *new_len = s->len;
+    return 0;
+  }
+  return kErrUnknown;
+}
+
+int query_prefix64(Session* s, size_t limit, long long* kept, long long* last) {
+  *kept = 0;
+  *last = -1;
+  if (s->q_kind == 0 || s->q_kind == 1) return 0;
+  const unsigned long long lim = std::min<unsigned long long>(limit, s->q_n);
+  if (lim == 0) return 0;
+  if (s->q_kind == 3) {  // empty pattern: an (empty) match at every position 0..n
+    *kept = (long long)lim;
+    *last = (long long)lim - 1;
+    return 0;
+  }
+  const unsigned long long t = lim / crb::kTile, rel = lim % crb::kTile;
+  cudaError_t e;
+  if (rel == 0) {
+    TileIncl ti;
+    e = cudaMemcpyAsync(&ti, s->incl + (t - 1), sizeof(TileIncl), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return (int)e;
+    *kept = (long long)ti.kept;
+    *last = ti.last;
+    return 0;
+  }
+  ReplaceParams p = s->q_params;
+  p.in = s->alt;  // the input of the last apply
+  p.query_tile = (uint32_t)t;
+  p.query_limit = (uint32_t)rel;
+  e = crb::launch_query(p, s->stream);
+  if (e != cudaSuccess) return (int)e;
+  ++s->launches;
+  e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return (int)e;
+  if (s->res_host->error_epoch == p.epoch) return kErrUnknown;
+  *kept = (long long)s->res_host->q_kept;
+  *last = s->res_host->q_last;
+  return 0;
+}
+
+int result_to_pinned(Session* s, uint8_t** out_host, size_t* outlen) {
+  *out_host = nullptr;
+  *outlen = s->len;
+  if (s->len == 0) return 0;
+  cudaError_t e;
+  void* host = pinned_pool().get(s->len, &e);
+  if (!host) {
+    *outlen = 0;
+    return (int)e;
+  }
+  e = cudaMemcpyAsync(host, s->buf, s->len, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) {
+    pinned_pool().put(host);
+    *outlen = 0;
+    return (int)e;
+  }
+  *out_host = (uint8_t*)host;
+  return 0;
+}
+
+// Idle sessions reused by cuda_replace_unified, so a one-shot call pays no allocation.
+std::mutex g_cache_mu;
+std::vector<Session*> g_cache;
+
+Session* cache_take(int device) {
+  std::lock_guard<std::mutex> g(g_cache_mu);
+  for (size_t i = 0; i < g_cache.size(); ++i) {
+    if (g_cache[i]->device == device) {
+      Session* s = g_cache[i];
+      g_cache.erase(g_cache.begin() + i);
+      return s;
+    }
+  }
+  return nullptr;
+}
+
+void cache_give(Session* s) {
+  {
+    std::lock_guard<std::mutex> g(g_cache_mu);
+    if (g_cache.size() < 8) {
+      g_cache.push_back(s);
+      return;
+    }
+  }
+  session_free(s);
+}
+
+#define SESSION_GUARD(h)                              \
+  if (!(h)) return -1;                                \
+  Session* s = static_cast<Session*>(h);              \
+  std::lock_guard<std::mutex> lock_(s->mtx);          \
+  if (!s->alive) return -3;                           \
+  cudaSetDevice(s->device)
+
+}  // namespace
+
+CR_EXPORT const char* cuda_replace_version(void) { return "cuda_replace_b200 1.0 sm_100a single-pass look-back"; }
+
+CR_EXPORT void cuda_free_host(void* p) {
+  if (p) pinned_pool().put(p);
+}
+
+CR_EXPORT int cuda_replace_open(void** ph, const uint8_t* src, size_t len) {
+  if (!ph) return -1;
+  *ph = nullptr;
+  Session* s = nullptr;
+  int rc = session_create(&s);
+  if (rc != 0) return rc;
+  rc = session_load(s, src, len);
+  if (rc != 0) {
+    session_free(s);
+    return rc;
+  }
+  *ph = s;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_reset(void* h, const uint8_t* src, size_t len) {
+  SESSION_GUARD(h);
+  return session_load(s, src, len);
+}
+
+CR_EXPORT int cuda_replace_build_index(void* h, size_t chunk_size) {
+  (void)chunk_size;
+  SESSION_GUARD(h);
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_apply(void* h, const uint8_t* pat, int pat_len, const uint8_t* rep, int rep_len,
+                                 size_t* new_len) {
+  SESSION_GUARD(h);
+  return apply_one(s, pat, pat_len, rep, rep_len, 0, nullptr, new_len);
+}
+
+CR_EXPORT int cuda_replace_apply_seeded(void* h, const uint8_t* pat, int pat_len, const uint8_t* rep,
+                                        int rep_len, long long prev_last_rel, long long* out_last_rel,
+                                        size_t* new_len) {
+  SESSION_GUARD(h);
+  const long long b = (pat_len > 0) ? prev_last_rel + (long long)pat_len : 0;
+  const unsigned long long block_before = b > 0 ? (unsigned long long)b : 0ull;
+  long long last = -1;
+  const int rc = apply_one(s, pat, pat_len, rep, rep_len, block_before, &last, new_len);
+  if (rc == 0 && out_last_rel) *out_last_rel = last;
+  return rc;
+}
+
+CR_EXPORT int cuda_replace_query_prefix(void* h, size_t limit, int* kept_before_limit,
+                                        int* last_kept_before_limit) {
+  SESSION_GUARD(h);
+  long long k = 0, l = -1;
+  const int rc = query_prefix64(s, limit, &k, &l);
+  if (rc != 0) return rc;
+  if (k > 0x7FFFFFFFll || l > 0x7FFFFFFFll) return -5;
+  if (kept_before_limit) *kept_before_limit = (int)k;
+  if (last_kept_before_limit) *last_kept_before_limit = (int)l;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_query_prefix64(void* h, size_t limit, long long* kept_before_limit,
+                                          long long* last_kept_before_limit) {
+  SESSION_GUARD(h);
+  long long k = 0, l = -1;
+  const int rc = query_prefix64(s, limit, &k, &l);
+  if (rc != 0) return rc;
+  if (kept_before_limit) *kept_before_limit = k;
+  if (last_kept_before_limit) *last_kept_before_limit = l;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_apply_batch(void* h, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+                                       const int* rep_lens, int count, size_t* new_len) {
+  SESSION_GUARD(h);
+  for (int i = 0; i < count; ++i) {
+    const uint8_t* p = pats ? pats[i] : nullptr;
+    const uint8_t* r = reps ? reps[i] : nullptr;
+    const int pl = pat_lens ? pat_lens[i] : 0;
+    const int rl = rep_lens ? rep_lens[i] : 0;
+    const int rc = apply_one(s, p, pl, r, rl, 0, nullptr, nullptr);
+    if (rc != 0) return rc;
+  }
+  if (new_len) *new_len = s->len;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_result(void* h, uint8_t** out_host, size_t* outlen_host) {
+  if (!h || !out_host || !outlen_host) return -1;
+  SESSION_GUARD(h);
+  return result_to_pinned(s, out_host, outlen_host);
+}
+
+CR_EXPORT int cuda_replace_result_into(void* h, uint8_t* dst, size_t cap, size_t* len) {
+  SESSION_GUARD(h);
+  if (len) *len = s->len;
+  if (s->len == 0) return 0;
+  if (!dst) return -1;
+  if (cap < s->len) return (int)cudaErrorInvalidValue;
+  cudaError_t e = cudaMemcpyAsync(dst, s->buf, s->len, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  return (int)e;
+}
+
+CR_EXPORT int cuda_replace_length(void* h, size_t* len) {
+  if (!len) return -1;
+  SESSION_GUARD(h);
+  *len = s->len;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_stats(void* h, unsigned long long* kept_last_apply, unsigned long long* kernel_launches) {
+  SESSION_GUARD(h);
+  if (kept_last_apply) *kept_last_apply = s->kept_last;
+  if (kernel_launches) *kernel_launches = s->launches;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size_t n, const uint8_t* pat,
+                                               int pat_len, const uint8_t* rep, int rep_len, uint8_t* d_out,
+                                               size_t out_cap, void* stream) {
+  SESSION_GUARD(h);
+  if (pat_len <= 0 || rep_len < 0 || (size_t)pat_len > n) return -1;
+  if (pat_len > crb::kInlineMax || rep_len > crb::kInlineMax) return -4;
+  if ((n && !d_in) || !d_out || !pat || (rep_len && !rep)) return -1;
+  if (((uintptr_t)d_in & 15u) || ((uintptr_t)d_out & 15u)) return (int)cudaErrorInvalidValue;
+  const uint32_t L = (uint32_t)pat_len, R = (uint32_t)rep_len;
+  if (out_cap < output_bound(n, L, R)) return (int)cudaErrorInvalidValue;
+  ReplaceParams p;
+  memset(&p, 0, sizeof(p));
+  crb::prepare_pattern_fields(p, pat, L);
+  p.R = R;
+  const size_t tiles = (n + crb::kTile - 1) / crb::kTile;
+  if (tiles > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;
+  p.num_tiles = (uint32_t)tiles;
+  cudaError_t e = ensure_scratch(s, tiles, p.agg_entries);
+  if (e != cudaSuccess) return (int)e;
+  memcpy(p.pat, pat, L);
+  if (R) memcpy(p.rep, rep, R);
+  p.in = d_in;
+  p.out = d_out;
+  p.n = n;
+  p.out_cap = out_cap;
+  p.status = s->status;
+  p.incl = s->incl;
+  p.agg = s->agg;
+  p.res = s->res;
+  p.epoch = next_epoch(s);
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  e = crb::launch_replace(p, st, nullptr);
+  if (e != cudaSuccess) return (int)e;
+  ++s->launches;
+  s->async_stream = st;
+  s->async_epoch = p.epoch;
+  s->q_kind = 0;
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_device_result(void* h, size_t* out_len, unsigned long long* kept) {
+  SESSION_GUARD(h);
+  if (!s->async_epoch) return -1;
+  cudaStream_t st = s->async_stream ? s->async_stream : s->stream;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return (int)e;
+  const ApplyResult r = *s->res_host;
+  if (r.error_epoch == s->async_epoch || r.overflow_epoch == s->async_epoch) return kErrUnknown;
+  if (out_len) *out_len = (size_t)r.out_len;
+  if (kept) *kept = r.kept;
+  return 0;
+}
+
+CR_EXPORT void cuda_replace_close(void* h) {
+  if (!h) return;
+  Session* s = static_cast<Session*>(h);
+  {
+    std::lock_guard<std::mutex> lock(s->mtx);
+    if (!s->alive) return;
+    s->alive = false;
+  }
+  session_free(s);
+}
+
+CR_EXPORT int cuda_replace_unified(const uint8_t* src, size_t src_len, const uint8_t* pat, int pat_len,
+                                   const uint8_t* rep, int rep_len, uint8_t** out_host, size_t* out_len) {
+  if (!out_host || !out_len) return -1;
+  *out_host = nullptr;
+  *out_len = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  Session* s = cache_take(dev);
+  int rc = 0;
+  if (!s) {
+    rc = session_create(&s);
+    if (rc != 0) return rc;
+  }
+  rc = session_load(s, src, src_len);
+  if (rc == 0) rc = apply_one(s, pat, pat_len, rep, rep_len, 0, nullptr, nullptr);
+  if (rc == 0) rc = result_to_pinned(s, out_host, out_len);
+  if (rc == 0) {
+    cache_give(s);
+  } else {
+    session_free(s);
+    *out_host = nullptr;
+    *out_len = 0;
+  }
+  return rc;
+}

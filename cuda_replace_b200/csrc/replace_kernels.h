@@ -1,0 +1,100 @@
+// replace_kernels.h - launch interface between the session layer (capi.cu) and the
+// sm_100a kernels (replace_kernels.cu).
+//
+// One apply of (pattern P of length L, replacement R) over an input of n bytes is ONE
+// launch of replace_tiles_kernel. The input is cut into 16 KiB tiles; each CTA of a
+// persistent grid takes tiles in increasing order from an atomic counter, stages the
+// tile plus an (L-1)-byte halo in shared memory with a 1-D TMA bulk copy, finds the
+// candidate positions, publishes the tile's carry function, resolves its exact
+// carry-in with a decoupled look-back over the predecessors, and writes its output
+// bytes at a 64-bit offset with TMA bulk stores. The leftmost, non-overlapping rule
+// of bytes.replace is exact across every tile boundary; no second pass exists.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace crb {
+
+constexpr int kThreads = 256;               // threads per CTA
+constexpr int kWarps = kThreads / 32;
+constexpr int kSeg = 64;                    // input bytes owned by one thread
+constexpr int kTile = kThreads * kSeg;      // 16384 input bytes per tile
+constexpr int kOutWin = 16384;              // output staging window in shared memory
+constexpr int kInlineMax = 256;             // pattern/replacement bytes carried in the launch parameters
+constexpr uint32_t kMaxLen = 8192;          // longest pattern / replacement (CUDA_REPLACE_MAX_PATTERN)
+
+// Carry modes. The carry between two tiles is "blocked until": how many leading bytes
+// of the next tile are covered by a match kept earlier.
+//  kModeFree:  P has no proper border (or L == 1), so two occurrences never overlap and
+//              every occurrence is kept; the carry only tells which leading bytes are
+//              covered. A tile's function is carry_out(c) = max(c - kTile, lco).
+//  kModeSmall: P has a border and L <= 64: the tile function is a table over c in [0, L).
+//  kModeLarge: P has a border and L > 64: same table, built without the warp level.
+enum CarryMode : uint32_t { kModeFree = 0, kModeSmall = 1, kModeLarge = 2 };
+
+// Look-back state of tile t: status[t] = (epoch << 2) | state.
+enum TileState : uint32_t { kStAgg = 1, kStInc = 2 };
+
+struct TileIncl {                 // inclusive prefix through tile t
+  unsigned long long kept;        // matches kept in tiles [0, t]
+  long long last;                 // start of the last of them (input position) or -1
+  unsigned int carry;             // bytes of tile t+1 covered by a match kept in [0, t]
+  unsigned int pad;
+};
+
+struct ApplyResult {              // device-side result block of one session
+  unsigned long long out_len;     // written by the CTA that owns the last tile
+  unsigned long long kept;
+  long long last_kept;
+  unsigned int error_epoch;       // == epoch: a bounded wait gave up; results invalid
+  unsigned int overflow_epoch;    // == epoch: output did not fit in out_cap; nothing valid written
+  unsigned int tile_counter;      // dynamic tile scheduler, reset by the last CTA to exit
+  unsigned int done_ctas;
+  unsigned long long q_kept;      // query_prefix answer
+  long long q_last;
+  unsigned long long pad[2];
+};
+
+struct ReplaceParams {
+  const uint8_t* in;              // 16-byte aligned; readable up to round_up(n, 16)
+  uint8_t* out;                   // 16-byte aligned, out_cap bytes
+  unsigned long long n;
+  unsigned long long out_cap;
+  unsigned long long block_before;  // candidates starting before this position are not taken
+  unsigned long long stride_mask; // bits 0, L, 2L, ... below 64 (1 when L >= 64)
+  unsigned int L, R;
+  unsigned int mode;              // CarryMode
+  unsigned int num_tiles;
+  unsigned int epoch;
+  unsigned int agg_entries;       // entries per tile function (1 in kModeFree, min(L, kTile) otherwise)
+  unsigned int p4, m4;            // first min(L, 4) pattern bytes (little endian) and their byte mask
+  unsigned int inv_l;             // ceil(65536 / L), for L < 64
+  unsigned int query_limit;       // query kernel: tile-relative limit
+  unsigned int query_tile;        // query kernel: tile index
+  unsigned int pad0;
+  unsigned int* status;           // [num_tiles]
+  TileIncl* incl;                 // [num_tiles]
+  unsigned long long* agg;        // [num_tiles * agg_entries]
+  ApplyResult* res;
+  const uint8_t* pat_ext;         // device copy when L > kInlineMax
+  const uint8_t* rep_ext;         // device copy when R > kInlineMax
+  uint8_t pat[kInlineMax];
+  uint8_t rep[kInlineMax];
+};
+
+// Host helpers (replace_kernels.cu).
+// Fills the pattern-derived fields of p (mode, p4, m4, inv_l, stride_mask, agg_entries).
+void prepare_pattern_fields(ReplaceParams& p, const uint8_t* pat, uint32_t L);
+// Dynamic shared memory bytes used by replace_tiles_kernel for (mode, L, R).
+uint32_t tile_kernel_smem_bytes(uint32_t mode, uint32_t L, uint32_t R);
+// Launch one apply. grid_ctas_out receives the number of CTAs launched.
+cudaError_t launch_replace(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out);
+// One CTA answers query_prefix for tile p.query_tile at tile-relative limit p.query_limit,
+// using the tile records of the apply described by p; writes res->q_kept / res->q_last.
+cudaError_t launch_query(const ReplaceParams& p, cudaStream_t st);
+// bytes.replace with an empty pattern: rep before every byte and at the end.
+cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const uint8_t* rep_dev,
+                                 uint32_t R, uint8_t* out, cudaStream_t st);
+
+}  // namespace crb

@@ -1,0 +1,293 @@
+"""ctypes binding of libcuda_replace.so with the interface of the reference wrapper.
+
+Same names, arguments, return values and errors as RAZZULLIX/cuda_replace's
+cuda_replace_wrapper.py (``CudaReplaceLib.unified`` py:124-141, ``Session`` py:145-297,
+``replace_unified`` py:301-303, ``gpu_replace_streaming`` py:305-366), so code written
+against the reference runs unchanged. Every call goes to the CUDA library; there is no CPU
+path, and loading fails loudly when the library has not been built.
+
+``gpu_replace_streaming`` keeps its signature but not the reference body: the reference
+cuts each chunk's output at ``(base_end-pos) + kept_before*diff`` (py:356), which drops the
+replacement of a match that straddles the chunk boundary and re-emits the bytes it covers.
+The version here cuts after that replacement and drops the covered bytes at the start of
+the next chunk, so the result equals the chained ``bytes.replace`` for any chunk size.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+_PKG_DIR = Path(__file__).resolve().parent
+DEFAULT_LIB = _PKG_DIR / "libcuda_replace.so"
+
+c_size_t = C.c_size_t
+c_uint8_p = C.POINTER(C.c_uint8)
+c_void_p = C.c_void_p
+c_int_p = C.POINTER(C.c_int)
+c_longlong_p = C.POINTER(C.c_longlong)
+c_size_t_p = C.POINTER(c_size_t)
+c_uint8_pp = C.POINTER(c_uint8_p)
+
+
+def _bind(lib: C.CDLL, name: str, argtypes, restype, optional: bool = False) -> None:
+    if optional and not hasattr(lib, name):
+        setattr(lib, name, None)  # additive entry point absent from this build
+        return
+    fn = getattr(lib, name)
+    fn.argtypes = argtypes
+    fn.restype = restype
+
+
+class CudaReplaceLib:
+    """Loads libcuda_replace.so and binds its C ABI (reference: py:36-141)."""
+
+    def __init__(self, dll_path: Optional[str] = None):
+        path = Path(os.fspath(dll_path)) if dll_path else DEFAULT_LIB
+        if not path.exists():
+            raise FileNotFoundError(
+                f"{path} not found: build it with `python -m cuda_replace_b200.build` "
+                "(the replace path has no CPU fallback)")
+        self.path = str(path)
+        self.lib = C.CDLL(self.path)
+        lib = self.lib
+        _bind(lib, "cuda_replace_unified",
+              [c_uint8_p, c_size_t, c_uint8_p, C.c_int, c_uint8_p, C.c_int, C.POINTER(c_uint8_p), c_size_t_p],
+              C.c_int)
+        _bind(lib, "cuda_free_host", [c_void_p], None)
+        _bind(lib, "cuda_replace_open", [C.POINTER(c_void_p), c_uint8_p, c_size_t], C.c_int)
+        _bind(lib, "cuda_replace_build_index", [c_void_p, c_size_t], C.c_int)
+        _bind(lib, "cuda_replace_apply", [c_void_p, c_uint8_p, C.c_int, c_uint8_p, C.c_int, c_size_t_p], C.c_int)
+        _bind(lib, "cuda_replace_apply_batch",
+              [c_void_p, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t_p], C.c_int)
+        _bind(lib, "cuda_replace_result", [c_void_p, C.POINTER(c_uint8_p), c_size_t_p], C.c_int)
+        _bind(lib, "cuda_replace_close", [c_void_p], None)
+        _bind(lib, "cuda_replace_reset", [c_void_p, c_uint8_p, c_size_t], C.c_int)
+        _bind(lib, "cuda_replace_apply_seeded",
+              [c_void_p, c_uint8_p, C.c_int, c_uint8_p, C.c_int, C.c_longlong, c_longlong_p, c_size_t_p],
+              C.c_int)
+        _bind(lib, "cuda_replace_query_prefix", [c_void_p, c_size_t, c_int_p, c_int_p], C.c_int)
+        _bind(lib, "cuda_replace_version", [], C.c_char_p)
+        # additive entry points
+        _bind(lib, "cuda_replace_length", [c_void_p, c_size_t_p], C.c_int)
+        _bind(lib, "cuda_replace_query_prefix64", [c_void_p, c_size_t, c_longlong_p, c_longlong_p], C.c_int)
+        _bind(lib, "cuda_replace_result_into", [c_void_p, c_void_p, c_size_t, c_size_t_p], C.c_int)
+        _bind(lib, "cuda_replace_stats",
+              [c_void_p, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)], C.c_int)
+        _bind(lib, "cuda_replace_apply_device_async",
+              [c_void_p, c_void_p, c_size_t, c_uint8_p, C.c_int, c_uint8_p, C.c_int, c_void_p, c_size_t, c_void_p],
+              C.c_int, optional=True)
+        _bind(lib, "cuda_replace_device_result", [c_void_p, c_size_t_p, C.POINTER(C.c_ulonglong)], C.c_int,
+              optional=True)
+
+    def version(self) -> str:
+        return self.lib.cuda_replace_version().decode()
+
+    def unified(self, src: bytes, pat: bytes, rep: bytes) -> bytes:
+        """One-shot replace (reference: py:124-141)."""
+        src_buf = C.create_string_buffer(src, len(src) or 1)
+        pat_buf = C.create_string_buffer(pat, len(pat) or 1)
+        rep_buf = C.create_string_buffer(rep, len(rep) or 1)
+        out_ptr = c_uint8_p()
+        out_len = c_size_t()
+        rc = self.lib.cuda_replace_unified(
+            C.cast(src_buf, c_uint8_p), c_size_t(len(src)),
+            C.cast(pat_buf, c_uint8_p), C.c_int(len(pat)),
+            C.cast(rep_buf, c_uint8_p), C.c_int(len(rep)),
+            C.byref(out_ptr), C.byref(out_len))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_unified failed rc={rc}")
+        try:
+            return C.string_at(out_ptr, out_len.value) if out_len.value else b""
+        finally:
+            self.lib.cuda_free_host(out_ptr)
+
+
+class Session:
+    """A device-resident buffer that successive replaces transform in place (reference: py:145-297)."""
+
+    def __init__(self, lib: CudaReplaceLib, src: bytes):
+        self.lib = lib
+        self.h = c_void_p()
+        buf = C.create_string_buffer(src, len(src) or 1)
+        rc = lib.lib.cuda_replace_open(C.byref(self.h), C.cast(buf, c_uint8_p), c_size_t(len(src)))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_open failed rc={rc}")
+
+    def __enter__(self) -> "Session":
+        return self
+
+    def __exit__(self, exc_type, exc, tb):
+        self.close()
+
+    def reset(self, src: bytes) -> None:
+        buf = C.create_string_buffer(src, len(src) or 1)
+        rc = self.lib.lib.cuda_replace_reset(self.h, C.cast(buf, c_uint8_p), c_size_t(len(src)))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_reset failed rc={rc}")
+
+    def build_index(self, chunk_size: Optional[int] = None) -> None:
+        rc = self.lib.lib.cuda_replace_build_index(self.h, c_size_t(0 if chunk_size is None else int(chunk_size)))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_build_index failed rc={rc}")
+
+    def apply(self, pat: bytes, rep: bytes) -> int:
+        pb = C.create_string_buffer(pat, len(pat) or 1)
+        rb = C.create_string_buffer(rep, len(rep) or 1)
+        new_len = c_size_t()
+        rc = self.lib.lib.cuda_replace_apply(self.h, C.cast(pb, c_uint8_p), C.c_int(len(pat)),
+                                             C.cast(rb, c_uint8_p), C.c_int(len(rep)), C.byref(new_len))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_apply failed rc={rc}")
+        return int(new_len.value)
+
+    def apply_seeded(self, pat: bytes, rep: bytes, prev_last_rel: int) -> Tuple[int, int]:
+        """Apply with carry-in; returns (new_len, last kept start in this buffer or -1)."""
+        pb = C.create_string_buffer(pat, len(pat) or 1)
+        rb = C.create_string_buffer(rep, len(rep) or 1)
+        new_len = c_size_t()
+        last = C.c_longlong(-1)
+        rc = self.lib.lib.cuda_replace_apply_seeded(
+            self.h, C.cast(pb, c_uint8_p), C.c_int(len(pat)), C.cast(rb, c_uint8_p), C.c_int(len(rep)),
+            C.c_longlong(int(prev_last_rel)), C.byref(last), C.byref(new_len))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_apply_seeded failed rc={rc}")
+        return int(new_len.value), int(last.value)
+
+    def apply_batch(self, pairs: Sequence[Tuple[bytes, bytes]]) -> int:
+        count = len(pairs)
+        if count == 0:
+            return self.length()
+        keep = []
+        pat_ptrs = (c_uint8_p * count)()
+        rep_ptrs = (c_uint8_p * count)()
+        pat_lens = (C.c_int * count)()
+        rep_lens = (C.c_int * count)()
+        for i, (pat, rep) in enumerate(pairs):
+            pb = C.create_string_buffer(pat, len(pat) or 1)
+            rb = C.create_string_buffer(rep, len(rep) or 1)
+            keep += [pb, rb]
+            pat_ptrs[i] = C.cast(pb, c_uint8_p)
+            rep_ptrs[i] = C.cast(rb, c_uint8_p)
+            pat_lens[i] = len(pat)
+            rep_lens[i] = len(rep)
+        new_len = c_size_t()
+        rc = self.lib.lib.cuda_replace_apply_batch(
+            self.h, C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
+            C.cast(rep_ptrs, c_uint8_pp), C.cast(rep_lens, c_int_p), C.c_int(count), C.byref(new_len))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_apply_batch failed rc={rc}")
+        return int(new_len.value)
+
+    def query_prefix(self, limit: int) -> Tuple[int, int]:
+        """(kept starts before limit, last such start or -1) of the most recent apply."""
+        kept = C.c_longlong(0)
+        last = C.c_longlong(-1)
+        rc = self.lib.lib.cuda_replace_query_prefix64(self.h, c_size_t(int(limit)), C.byref(kept), C.byref(last))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_query_prefix failed rc={rc}")
+        return int(kept.value), int(last.value)
+
+    def result(self) -> bytes:
+        out_ptr = c_uint8_p()
+        out_len = c_size_t()
+        rc = self.lib.lib.cuda_replace_result(self.h, C.byref(out_ptr), C.byref(out_len))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_result failed rc={rc}")
+        try:
+            return C.string_at(out_ptr, out_len.value) if out_len.value else b""
+        finally:
+            self.lib.lib.cuda_free_host(out_ptr)
+
+    def length(self) -> int:
+        n = c_size_t()
+        rc = self.lib.lib.cuda_replace_length(self.h, C.byref(n))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_length failed rc={rc}")
+        return int(n.value)
+
+    def stats(self) -> Tuple[int, int]:
+        kept, launches = C.c_ulonglong(0), C.c_ulonglong(0)
+        rc = self.lib.lib.cuda_replace_stats(self.h, C.byref(kept), C.byref(launches))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_stats failed rc={rc}")
+        return int(kept.value), int(launches.value)
+
+    def apply_device_async(self, d_in: int, n: int, pat: bytes, rep: bytes, d_out: int, out_cap: int,
+                           stream: int = 0) -> None:
+        """Enqueue a replace of device memory d_in[0, n) into d_out on a CUDA stream handle."""
+        pb = C.create_string_buffer(pat, len(pat) or 1)
+        rb = C.create_string_buffer(rep, len(rep) or 1)
+        rc = self.lib.lib.cuda_replace_apply_device_async(
+            self.h, c_void_p(d_in), c_size_t(n), C.cast(pb, c_uint8_p), C.c_int(len(pat)),
+            C.cast(rb, c_uint8_p), C.c_int(len(rep)), c_void_p(d_out), c_size_t(out_cap), c_void_p(stream))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_apply_device_async failed rc={rc}")
+
+    def device_result(self) -> Tuple[int, int]:
+        """(output length, matches kept) of the last apply_device_async, after waiting for it."""
+        n, kept = c_size_t(0), C.c_ulonglong(0)
+        rc = self.lib.lib.cuda_replace_device_result(self.h, C.byref(n), C.byref(kept))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_device_result failed rc={rc}")
+        return int(n.value), int(kept.value)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.lib.cuda_replace_close(self.h)
+            self.h = c_void_p(None)
+
+
+def replace_unified(lib: CudaReplaceLib, src: bytes, pat: bytes, rep: bytes) -> bytes:
+    """One-shot convenience around cuda_replace_unified (reference: py:301-303)."""
+    return lib.unified(src, pat, rep)
+
+
+def stream_chunk_plan(n: int, chunk_bytes: int) -> List[Tuple[int, int]]:
+    """[pos, base_end) ranges of the chunks of an n-byte input."""
+    chunk_bytes = max(1, int(chunk_bytes))
+    return [(p, min(p + chunk_bytes, n)) for p in range(0, n, chunk_bytes)]
+
+
+def gpu_replace_streaming(lib: CudaReplaceLib, src: bytes, pairs: Iterable[Tuple[bytes, bytes]],
+                          chunk_bytes: int = 256 * 1024 * 1024) -> bytes:
+    """Chunked, pair-major replacement of an input larger than device memory
+    (reference signature: py:305-308). Each chunk carries an (L-1)-byte halo; the carry-in
+    is the start of the previous chunk's last kept match, passed to apply_seeded."""
+    out = src
+    with Session(lib, b"") as sess:
+        for pat, rep in pairs:
+            L = len(pat)
+            n = len(out)
+            pieces: List[bytes] = []
+            if L == 0:
+                # bytes.replace(b"", rep): rep before each byte and once at the end
+                plan = stream_chunk_plan(n, chunk_bytes)
+                for pos, base_end in plan:
+                    sess.reset(out[pos:base_end])
+                    sess.apply(pat, rep)
+                    piece = sess.result()
+                    pieces.append(piece[:len(piece) - len(rep)])
+                pieces.append(rep)
+                out = b"".join(pieces)
+                continue
+            diff = len(rep) - L
+            prev_last: Optional[int] = None  # global start of the last kept match so far
+            for pos, base_end in stream_chunk_plan(n, chunk_bytes):
+                take_end = min(base_end + L - 1, n)
+                sess.reset(out[pos:take_end])
+                seed = (prev_last - pos) if prev_last is not None else -(1 << 62)
+                sess.apply_seeded(pat, rep, seed)
+                limit = base_end - pos
+                kept_before, last_before = sess.query_prefix(limit)
+                chunk_out = sess.result()
+                # bytes covered by the previous chunk's last match were emitted as literals: drop
+                skip = max(0, prev_last + L - pos) if prev_last is not None else 0
+                overhang = max(0, last_before + L - limit) if kept_before else 0
+                end = limit + kept_before * diff + overhang
+                pieces.append(chunk_out[skip:end] if skip < end else b"")
+                if kept_before:
+                    prev_last = pos + last_before
+            out = b"".join(pieces)
+    return out

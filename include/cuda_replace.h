@@ -1,0 +1,150 @@
+/*
+ * cuda_replace.h - C ABI of libcuda_replace.so (B200 / sm_100a build).
+ *
+ * Leftmost, non-overlapping byte-pattern replacement with the semantics of
+ * Python's bytes.replace. The first twelve entry points keep the exact
+ * signatures, ownership rules and return codes of the RAZZULLIX/cuda_replace
+ * library (cuda_replace.cu), so the unchanged cuda_replace_wrapper.py binds this
+ * library through ctypes. Each declaration cites the reference export it
+ * replaces (cuda_replace.cu:<line>) and the ctypes binding that loads it
+ * (cuda_replace_wrapper.py:<line>).
+ *
+ * Return codes (all int-returning calls):
+ *    0   success
+ *   -1   null handle or null output argument
+ *   -2   the session object could not be allocated
+ *   -3   the handle has been closed
+ *   -4   pattern or replacement longer than CUDA_REPLACE_MAX_PATTERN
+ *   -5   a 32-bit output of cuda_replace_query_prefix cannot hold the value
+ *        (use cuda_replace_query_prefix64)
+ *   >0   a cudaError_t; 999 (cudaErrorUnknown) for internal failures, including a
+ *        bounded device-side wait that gave up
+ *
+ * Threading: calls on one handle are serialised by a per-handle mutex; different
+ * handles may be used concurrently from different threads. A handle must not be
+ * used after cuda_replace_close returns.
+ *
+ * Ownership: input buffers stay owned by the caller and are only read during the
+ * call. *out_host buffers are page-locked host memory owned by the library and are
+ * released with cuda_free_host. An empty result returns *out_host == NULL.
+ */
+#ifndef CUDA_REPLACE_H
+#define CUDA_REPLACE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Longest pattern and replacement accepted by every apply call. */
+#define CUDA_REPLACE_MAX_PATTERN 8192
+
+/* Library identification string.
+ * Replaces cuda_replace_version (cuda_replace.cu:2251). Not bound by the wrapper. */
+const char* cuda_replace_version(void);
+
+/* One-shot replace: upload src, replace every leftmost non-overlapping pat with rep,
+ * return the result in library-owned page-locked memory.
+ * Replaces cuda_replace_unified (cuda_replace.cu:2579);
+ * bound at cuda_replace_wrapper.py:48-54, called at cuda_replace_wrapper.py:124-141. */
+int cuda_replace_unified(const uint8_t* src, size_t src_len,
+                         const uint8_t* pat, int pat_len,
+                         const uint8_t* rep, int rep_len,
+                         uint8_t** out_host, size_t* out_len);
+
+/* Release a buffer returned through *out_host.
+ * Replaces cuda_free_host (cuda_replace.cu:2559); bound at cuda_replace_wrapper.py:57-58. */
+void cuda_free_host(void* p);
+
+/* Open a session whose device-resident buffer holds a copy of src[0, len).
+ * Replaces cuda_replace_open (cuda_replace.cu:2256); bound at cuda_replace_wrapper.py:61-62. */
+int cuda_replace_open(void** ph, const uint8_t* src, size_t len);
+
+/* Replace the session buffer with a copy of src[0, len), reusing device capacity.
+ * Replaces cuda_replace_reset (cuda_replace.cu:2295); bound at cuda_replace_wrapper.py:97-101. */
+int cuda_replace_reset(void* h, const uint8_t* src, size_t len);
+
+/* Accepted for compatibility and does nothing: the reference builds a presence index
+ * here that no apply path consults (cuda_replace.cu:1249, 1904, 2006).
+ * Replaces cuda_replace_build_index (cuda_replace.cu:2320); bound at cuda_replace_wrapper.py:65-69. */
+int cuda_replace_build_index(void* h, size_t chunk_size);
+
+/* Replace every leftmost non-overlapping occurrence of pat in the session buffer.
+ * *new_len receives the new buffer length.
+ * Replaces cuda_replace_apply (cuda_replace.cu:2356); bound at cuda_replace_wrapper.py:73-76. */
+int cuda_replace_apply(void* h, const uint8_t* pat, int pat_len,
+                       const uint8_t* rep, int rep_len, size_t* new_len);
+
+/* As cuda_replace_apply, with a carry-in: prev_last_rel is the start of the previous
+ * kept match relative to byte 0 of this buffer (negative when it lies in an earlier
+ * chunk), so candidates starting before prev_last_rel + pat_len are not taken. The
+ * bytes that match covers inside this buffer are still emitted as literals (the
+ * previous chunk already emitted its replacement). *out_last_rel receives the start of
+ * the last match kept in this buffer, or -1.
+ * Replaces cuda_replace_apply_seeded (cuda_replace.cu:2403); bound at cuda_replace_wrapper.py:104-114. */
+int cuda_replace_apply_seeded(void* h, const uint8_t* pat, int pat_len,
+                              const uint8_t* rep, int rep_len,
+                              long long prev_last_rel, long long* out_last_rel,
+                              size_t* new_len);
+
+/* Over the matches kept by the most recent apply (positions in that apply's input):
+ * *kept_before_limit = how many start before limit, *last_kept_before_limit = the
+ * last such start or -1. limit is clamped to that input's length.
+ * Replaces cuda_replace_query_prefix (cuda_replace.cu:2452); bound at cuda_replace_wrapper.py:117-121. */
+int cuda_replace_query_prefix(void* h, size_t limit, int* kept_before_limit,
+                              int* last_kept_before_limit);
+
+/* Apply count (pattern, replacement) pairs in order, each to the output of the previous.
+ * Replaces cuda_replace_apply_batch (cuda_replace.cu:2465); bound at cuda_replace_wrapper.py:79-87. */
+int cuda_replace_apply_batch(void* h, const uint8_t** pats, const int* pat_lens,
+                             const uint8_t** reps, const int* rep_lens,
+                             int count, size_t* new_len);
+
+/* Copy the session buffer to library-owned page-locked memory (free with cuda_free_host).
+ * Replaces cuda_replace_result (cuda_replace.cu:2528); bound at cuda_replace_wrapper.py:90-91. */
+int cuda_replace_result(void* h, uint8_t** out_host, size_t* outlen_host);
+
+/* Close the session and free its device memory.
+ * Replaces cuda_replace_close (cuda_replace.cu:2565); bound at cuda_replace_wrapper.py:94-95. */
+void cuda_replace_close(void* h);
+
+/* ---- Additive entry points (no counterpart in the reference; optional for callers) ---- */
+
+/* Current length of the session buffer, without copying it to the host. */
+int cuda_replace_length(void* h, size_t* len);
+
+/* 64-bit form of cuda_replace_query_prefix. */
+int cuda_replace_query_prefix64(void* h, size_t limit, long long* kept_before_limit,
+                                long long* last_kept_before_limit);
+
+/* Copy the session buffer into caller memory dst[0, cap). *len receives the length;
+ * returns cudaErrorInvalidValue (1) when cap is too small (nothing is copied). */
+int cuda_replace_result_into(void* h, uint8_t* dst, size_t cap, size_t* len);
+
+/* Device-side counters of the most recent apply on this handle: number of matches kept
+ * and the number of kernel launches issued by this library since the handle was opened. */
+int cuda_replace_stats(void* h, unsigned long long* kept_last_apply,
+                       unsigned long long* kernel_launches);
+
+/* Replace in device memory: d_in[0, n) -> d_out, enqueued on `stream` (a cudaStream_t;
+ * NULL = the session's own stream) without waiting for it. d_in and d_out must be 16-byte
+ * aligned device pointers, d_in readable up to n rounded up to 16, and out_cap at least
+ * the worst-case output n + (n / pat_len) * max(0, rep_len - pat_len). pat_len must be in
+ * [1, 256] and rep_len in [0, 256]. Calls on one handle must use one stream (they share the
+ * handle's look-back scratch). The session buffer is not touched. */
+int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size_t n,
+                                    const uint8_t* pat, int pat_len,
+                                    const uint8_t* rep, int rep_len,
+                                    uint8_t* d_out, size_t out_cap, void* stream);
+
+/* Wait for the last cuda_replace_apply_device_async of this handle and report its output
+ * length and number of matches kept. */
+int cuda_replace_device_result(void* h, size_t* out_len, unsigned long long* kept);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDA_REPLACE_H */

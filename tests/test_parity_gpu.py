@@ -1,0 +1,196 @@
+"""Parity of libcuda_replace.so (sm_100a) with the oracle: CPython bytes.replace, chained
+per pair, and the C restatement for seeded applies and prefix queries. Every call goes
+through the C ABI. Bit-exact is the only acceptable result."""
+import hashlib
+import json
+import random
+from pathlib import Path
+
+import pytest
+
+from cuda_replace_b200 import cuda_replace_wrapper as Wr
+from cuda_replace_b200 import workloads as WL
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "vectors.json").read_text())
+TILE = 16384
+
+
+def sha(b):
+    return hashlib.sha256(b).hexdigest()
+
+
+def recipe_bytes(recipe):
+    return b"".join(bytes.fromhex(u) * c for u, c in recipe)
+
+
+def chain(src, pairs):
+    for p, r in pairs:
+        src = src.replace(p, r)
+    return src
+
+
+@pytest.mark.parametrize("row", GOLDEN["known_answer"] + GOLDEN["defects"], ids=lambda r: r["name"])
+def test_golden_vectors(cr_lib, row):
+    src = recipe_bytes(row["recipe"])
+    pairs = [(bytes.fromhex(p), bytes.fromhex(r)) for p, r in row["pairs"]]
+    if len(pairs) == 1:
+        out = cr_lib.unified(src, *pairs[0])
+        assert len(out) == row["out_len"] and sha(out) == row["out_sha256"]
+    with Wr.Session(cr_lib, src) as s:
+        for p, r in pairs:
+            s.apply(p, r)
+        out = s.result()
+    assert len(out) == row["out_len"] and sha(out) == row["out_sha256"]
+
+
+@pytest.mark.parametrize("row", GOLDEN["configs"], ids=lambda r: r["name"])
+def test_config_digests(cr_lib, row):
+    from tests.golden.make_golden import config_inputs
+    src, pairs = config_inputs(row)
+    with Wr.Session(cr_lib, src) as s:
+        n = s.apply_batch(pairs)
+        out = s.result()
+    assert n == row["out_len"] and len(out) == row["out_len"] and sha(out) == row["out_sha256"]
+
+
+def test_random_small_cases(cr_lib):
+    rng = random.Random(2024)
+    alphabets = [b"a", b"ab", b"aab", b"abc", b"\x00\x01", bytes(range(7))]
+    with Wr.Session(cr_lib, b"") as s:
+        for _ in range(1500):
+            alpha = rng.choice(alphabets)
+            src = bytes(rng.choice(alpha) for _ in range(rng.randint(0, 70)))
+            pat = bytes(rng.choice(alpha) for _ in range(rng.randint(0, 7)))
+            rep = bytes(rng.choice(b"XY\x00z") for _ in range(rng.randint(0, 9)))
+            s.reset(src)
+            n = s.apply(pat, rep)
+            out = s.result()
+            assert out == src.replace(pat, rep), (src, pat, rep, out)
+            assert n == len(out)
+
+
+PATTERNS = [b"a", b"aa", b"aaa", b"ab", b"aba", b"abab", b"ACGT", b"a" * 5, b"a" * 31, b"a" * 32,
+            b"a" * 33, b"a" * 63, b"a" * 64, b"a" * 65, b"ab" * 40, b"a" * 257, b"aab" * 100 + b"a",
+            b"xyz" * 90 + b"q"]
+
+
+@pytest.mark.parametrize("pat", PATTERNS, ids=lambda p: f"L{len(p)}-{p[:6]!r}")
+def test_periodic_runs_across_tiles(cr_lib, pat):
+    """Long runs where every position is a candidate: the carry between tiles decides
+    every kept start (the reference's tile-carry defect lives here)."""
+    sizes = [TILE - 1, TILE, TILE + 1, 3 * TILE + 17, 20000, 40001, 200_003]
+    with Wr.Session(cr_lib, b"") as s:
+        for n in sizes:
+            for base in (b"a", b"ab", b"aab"):
+                src = (base * (n // len(base) + 1))[:n]
+                for rep in (b"", b"X", b"QRS", b"0123456789" * 3):
+                    s.reset(src)
+                    s.apply(pat, rep)
+                    assert s.result() == src.replace(pat, rep), (n, base, pat[:8], len(pat), rep)
+
+
+def test_tile_boundary_straddles(cr_lib):
+    rng = random.Random(5)
+    for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
+        pat = bytes(rng.randrange(256) for _ in range(L))
+        src = bytearray(rng.randrange(256) for _ in range(5 * TILE + 77))
+        for b in range(TILE, len(src) - L, TILE):
+            for off in (1, L // 2, L - 1):
+                s0 = b - off
+                src[s0:s0 + L] = pat
+        src = bytes(src)
+        for rep in (b"", b"#", bytes(L + 7)):
+            assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep)
+
+
+def test_expansion_windows(cr_lib):
+    # each 16 KiB input tile expands to ~3.2 MB of output: many output windows per tile
+    src = b"a" * (3 * TILE + 5) + b"b" * 1000
+    for rep in (b"x" * 200, bytes(range(256)) * 20):
+        assert cr_lib.unified(src, b"a", rep) == src.replace(b"a", rep)
+
+
+def test_long_patterns_and_replacements(cr_lib):
+    rng = random.Random(11)
+    for L, R in ((257, 3), (300, 8192), (1000, 1), (4096, 4096), (8192, 0), (8192, 8192)):
+        pat = bytes(rng.randrange(256) for _ in range(L))
+        rep = bytes(rng.randrange(256) for _ in range(R))
+        filler = bytes(rng.randrange(256) for _ in range(3 * L + 100))
+        src = filler + pat + pat + filler[:L // 2] + pat + filler
+        assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep)
+    # bordered long pattern over a periodic text (tile tables beyond the warp level)
+    pat = b"ab" * 300
+    src = b"ab" * 40000
+    assert cr_lib.unified(src, pat, b"Z") == src.replace(pat, b"Z")
+
+
+def test_too_long_pattern_is_rejected(cr_lib):
+    with Wr.Session(cr_lib, b"abc") as s:
+        with pytest.raises(RuntimeError, match="rc=-4"):
+            s.apply(b"p" * 8193, b"")
+
+
+def test_seeded_apply_and_query_prefix(cr_lib, oracle_mod):
+    rng = random.Random(77)
+    with Wr.Session(cr_lib, b"") as s:
+        for trial in range(60):
+            base = rng.choice([b"a", b"ab", b"aab", b"abc"])
+            n = rng.choice([10, 100, TILE + 3, 3 * TILE, 70000])
+            src = bytearray((base * (n // len(base) + 1))[:n])
+            for _ in range(rng.randint(0, 20)):
+                src[rng.randrange(n)] = ord("z")
+            src = bytes(src)
+            pat = (base * 8)[:rng.randint(1, 6)]
+            rep = b"R" * rng.randint(0, 4)
+            seed = rng.choice([-(1 << 40), -(1 << 29), -3, -2, -1, 0, 5, n // 2])
+            s.reset(src)
+            new_len, last = s.apply_seeded(pat, rep, seed)
+            bb = oracle_mod.block_before_from_seed(seed, len(pat))
+            exp, kept, exp_last = oracle_mod.replace(src, pat, rep, bb)
+            assert s.result() == exp
+            assert new_len == len(exp) and last == exp_last
+            for lim in sorted({0, 1, n // 3, n // 2, TILE - 1, TILE, TILE + 1, n - 1, n, n + 5}):
+                if lim < 0:
+                    continue
+                assert s.query_prefix(lim) == oracle_mod.query_prefix(src, pat, lim, bb), (trial, lim)
+
+
+def test_query_prefix_int_abi(cr_lib):
+    import ctypes as C
+    with Wr.Session(cr_lib, b"abcabcabc") as s:
+        s.apply(b"abc", b"X")
+        k, l = C.c_int(0), C.c_int(0)
+        assert cr_lib.lib.cuda_replace_query_prefix(s.h, 7, C.byref(k), C.byref(l)) == 0
+        assert (k.value, l.value) == (3, 6)
+
+
+def test_streaming_helper_with_planted_straddles(cr_lib):
+    txt = WL.text_corpus(3 << 20, seed=4)
+    pairs = WL.c4_pairs(seed=4)
+    chunk = 256 << 10
+    for pat, _ in pairs[:3]:
+        txt, _count = WL.plant_across_boundaries(txt, pat, chunk, seed=len(pat))
+    assert Wr.gpu_replace_streaming(cr_lib, txt, pairs, chunk_bytes=chunk) == chain(txt, pairs)
+
+
+def test_c1_full_size(cr_lib):
+    data, pat, rep = WL.c1_acgt()
+    assert cr_lib.unified(data, pat, rep) == data.replace(pat, rep)
+
+
+def test_apply_batch_empty_and_null_pairs(cr_lib):
+    with Wr.Session(cr_lib, b"hello") as s:
+        assert s.apply_batch([]) == 5
+        assert s.apply_batch([(b"", b"-"), (b"-h", b"H")]) == 10
+        assert s.result() == b"hello".replace(b"", b"-").replace(b"-h", b"H")
+
+
+def test_launch_counter_counts_kernels(cr_lib):
+    with Wr.Session(cr_lib, b"a" * 100000) as s:
+        _, l0 = s.stats()
+        s.apply(b"aa", b"b")
+        s.apply(b"b", b"cc")
+        kept, l1 = s.stats()
+        assert l1 - l0 == 2 and kept == 50000
