@@ -17,6 +17,7 @@
  *   -4   pattern or replacement longer than CUDA_REPLACE_MAX_PATTERN
  *   -5   a 32-bit output of cuda_replace_query_prefix cannot hold the value
  *        (use cuda_replace_query_prefix64)
+ *   -6   a size above the fixed limits of cuda_replace_apply_device_noalloc
  *   >0   a cudaError_t; 999 (cudaErrorUnknown) for internal failures, including a
  *        bounded device-side wait that gave up
  *
@@ -142,6 +143,25 @@ int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size_t n,
 /* Wait for the last cuda_replace_apply_device_async of this handle and report its output
  * length and number of matches kept. */
 int cuda_replace_device_result(void* h, size_t* out_len, unsigned long long* kept);
+
+/* No counterpart in the reference. For callers that must not allocate memory at call time
+ * (an arena or pool owns the device budget, a host forbids cudaMalloc/cudaFree because they
+ * can synchronise the device, or the path must not fail on out-of-memory): replace
+ * d_in[0, n) into d_out with no allocation at all. The kernel's scratch is a fixed
+ * __device__ array of about 2.1 MiB that every GPU loading this library keeps until exit.
+ * Limits: n <= CUDA_REPLACE_NOALLOC_MAX_INPUT, pat_len in [1, 64], rep_len in [0, 256]
+ * (else -6); d_in and d_out 16-byte aligned, d_in readable up to n rounded up to 16, and
+ * out_cap >= n + (n / pat_len) * max(0, rep_len - pat_len) (else 1). Runs on `stream`
+ * (a cudaStream_t, NULL = default stream) and waits for it; *out_len gets the output length.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current; make that first call before any stream capture. All calls on
+ * a device share the array: calls whose work overlaps on the GPU race and must not be made. */
+#define CUDA_REPLACE_NOALLOC_MAX_INPUT (64u << 20)
+int cuda_replace_apply_device_noalloc(const uint8_t* d_in, size_t n,
+                                      const uint8_t* pat, int pat_len,
+                                      const uint8_t* rep, int rep_len,
+                                      uint8_t* d_out, size_t out_cap, size_t* out_len,
+                                      void* stream);
 
 #ifdef __cplusplus
 }
