@@ -49,6 +49,7 @@ def parse_args(argv=None):
     ap.add_argument("--scale", type=float, default=1.0, help="input size multiplier (1.0 = full size)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cases", default="0,1,2", help="comma-separated subset of the three cases (profiling)")
     return ap.parse_args(argv)
 
 
@@ -256,13 +257,17 @@ def run_ours(args, dist: Dist):
             torch.empty(n_rand + 64, dtype=torch.uint8, device=dev)]
     caps = [n_run, 3 * n_run, n_rand]
     ins = [(d_run, n_run), (d_run, n_run), (d_rand, n_rand)]
-    stream = torch.cuda.Stream(device=dev)
-    sessions = [Session(lib, b"") for _ in CASES]
-
     exp = expected_lengths(n_run, rand_np.tobytes()) if dist.rank == 0 else None
+    sel = [int(c) for c in args.cases.split(",")]
+    cases = [CASES[i] for i in sel]
+    outs, caps, ins = [outs[i] for i in sel], [caps[i] for i in sel], [ins[i] for i in sel]
+    if exp is not None:
+        exp = [exp[i] for i in sel]
+    stream = torch.cuda.Stream(device=dev)
+    sessions = [Session(lib, b"") for _ in cases]
 
     def one_step(events=None):
-        for i, ((name, pat, rep), (d_in, n), out, cap, s) in enumerate(zip(CASES, ins, outs, caps, sessions)):
+        for i, ((name, pat, rep), (d_in, n), out, cap, s) in enumerate(zip(cases, ins, outs, caps, sessions)):
             if events is not None:
                 events[i][0].record(stream)
             s.apply_device_async(d_in.data_ptr(), n, pat, rep, out.data_ptr(), cap, stream.cuda_stream)
@@ -276,14 +281,14 @@ def run_ours(args, dist: Dist):
     # correctness of the warm-up outputs (lengths + kept counts) against the oracle
     results = [s.device_result() for s in sessions]
     if exp is not None:
-        for (name, _, _), got, want in zip(CASES, results, exp):
+        for (name, _, _), got, want in zip(cases, results, exp):
             if tuple(got) != tuple(want):
                 raise SystemExit(f"bench self-check failed for {name}: got {got}, want {want}")
     bytes_per_step = sum(n + r[0] for (_, n), r in zip(ins, results))
     launches0 = sum(s.stats()[1] for s in sessions)
 
     per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                   for _ in CASES] for _ in range(args.steps)]
+                   for _ in cases] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(dist.local_rank)
     dist.barrier()
@@ -304,7 +309,7 @@ def run_ours(args, dist: Dist):
 
     # roofline of the replace kernel: algorithmic (in+out) bytes / mean launch duration
     launch_ms = [[per_launch[k][i][0].elapsed_time(per_launch[k][i][1]) for k in range(args.steps)]
-                 for i in range(len(CASES))]
+                 for i in range(len(cases))]
     case_bytes = [n + r[0] for (_, n), r in zip(ins, results)]
     achieved = sum(case_bytes) / (sum(statistics.mean(m) for m in launch_ms) / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
@@ -313,7 +318,7 @@ def run_ours(args, dist: Dist):
     # e2e through the reference-facing C ABI with page-locked host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, lib, n_run, rand_np, dist, dev)
+        e2e = run_e2e(args, lib, n_run, rand_np, dist, dev, sel)
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
@@ -334,7 +339,7 @@ def run_ours(args, dist: Dist):
                 "bytes_in_plus_out_per_step": bytes_per_step, "l2": "inputs larger than L2 (126 MB), no flush",
                 "parallelism": f"replicas x{dist.world}",
                 "per_case_gbs": {c[0]: round(b / (statistics.mean(m) / 1e3) / 1e9, 1)
-                                 for c, b, m in zip(CASES, case_bytes, launch_ms)},
+                                 for c, b, m in zip(cases, case_bytes, launch_ms)},
             },
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
@@ -353,15 +358,15 @@ def run_ours(args, dist: Dist):
     return 0
 
 
-def run_e2e(args, lib, n_run, rand_np, dist: Dist, dev):
+def run_e2e(args, lib, n_run, rand_np, dist: Dist, dev, sel):
     import torch
     h_run = torch.full((n_run,), ord("a"), dtype=torch.uint8).pin_memory()
     h_rand = torch.from_numpy(rand_np).pin_memory()
-    srcs = [(h_run, n_run), (h_run, n_run), (h_rand, len(rand_np))]
+    srcs = [[(h_run, n_run), (h_run, n_run), (h_rand, len(rand_np))][i] for i in sel]
     out_ptr = C.POINTER(C.c_uint8)()
     out_len = C.c_size_t()
     pats = [(C.create_string_buffer(p, len(p) or 1), len(p), C.create_string_buffer(r, len(r) or 1), len(r))
-            for _, p, r in CASES]
+            for _, p, r in (CASES[i] for i in sel)]
 
     def step():
         h2d = d2h = 0

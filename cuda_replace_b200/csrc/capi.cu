@@ -122,6 +122,7 @@ struct Session {
   size_t tiles_cap = 0;
   unsigned long long* agg = nullptr;
   size_t agg_cap = 0;
+  long long* tile_last = nullptr;  // per super-tile (same capacity as status)
   ApplyResult* res = nullptr;       // device
   ApplyResult* res_host = nullptr;  // page-locked mirror
   uint8_t* ext = nullptr;           // device copy of long patterns / replacements
@@ -174,11 +175,18 @@ cudaError_t ensure_scratch(Session* s, size_t tiles, size_t entries_per_tile) {
     const size_t cap = tiles + tiles / 8 + 64;
     uint32_t* st = nullptr;
     TileIncl* in = nullptr;
+    long long* tl = nullptr;
     cudaError_t e = cudaMalloc(&st, cap * sizeof(uint32_t));
     if (e != cudaSuccess) return e;
     e = cudaMalloc(&in, cap * sizeof(TileIncl));
     if (e != cudaSuccess) {
       cudaFree(st);
+      return e;
+    }
+    e = cudaMalloc(&tl, cap * sizeof(long long));
+    if (e != cudaSuccess) {
+      cudaFree(st);
+      cudaFree(in);
       return e;
     }
     e = cudaMemsetAsync(st, 0, cap * sizeof(uint32_t), s->stream);
@@ -189,8 +197,10 @@ cudaError_t ensure_scratch(Session* s, size_t tiles, size_t entries_per_tile) {
     }
     if (s->status) cudaFree(s->status);
     if (s->incl) cudaFree(s->incl);
+    if (s->tile_last) cudaFree(s->tile_last);
     s->status = st;
     s->incl = in;
+    s->tile_last = tl;
     s->tiles_cap = cap;
   }
   const size_t entries = tiles * entries_per_tile;
@@ -223,6 +233,7 @@ void session_free(Session* s) {
   if (s->alt) cudaFree(s->alt);
   if (s->status) cudaFree(s->status);
   if (s->incl) cudaFree(s->incl);
+  if (s->tile_last) cudaFree(s->tile_last);
   if (s->agg) cudaFree(s->agg);
   if (s->res) cudaFree(s->res);
   if (s->res_host) cudaFreeHost(s->res_host);
@@ -310,6 +321,13 @@ void swap_buffers(Session* s) {
   std::swap(s->buf_cap, s->alt_cap);
 }
 
+// Start of the last kept match of the launch described by p (after it completed).
+long long last_kept_of(const ReplaceParams& p, const ApplyResult& r) {
+  if (!p.nsub) return r.last_kept;
+  if ((r.last_tagged >> 40) != (unsigned long long)p.epoch) return -1;
+  return (long long)(r.last_tagged & ((1ull << 40) - 1)) - 1;
+}
+
 // One apply. block_before: candidates starting before it are not taken.
 int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, int rep_len,
               unsigned long long block_before, long long* out_last, size_t* new_len) {
@@ -359,11 +377,14 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
   memset(&p, 0, sizeof(p));
   crb::prepare_pattern_fields(p, pat, L);
   p.R = R;
-  const size_t tiles = (n + crb::kTile - 1) / crb::kTile;
+  p.nsub = crb::super_nsub(p.mode, L);
+  const size_t tile_bytes = (size_t)crb::kTile * (p.nsub ? p.nsub : 1u);
+  const size_t tiles = (n + tile_bytes - 1) / tile_bytes;
   if (tiles > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;
   p.num_tiles = (uint32_t)tiles;
   e = ensure_scratch(s, tiles, p.agg_entries);
   if (e != cudaSuccess) return (int)e;
+  p.tile_last = s->tile_last;
 
   const size_t bound = output_bound(n, L, R);
   size_t want = bound;
@@ -392,7 +413,7 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
     p.out = s->alt;
     p.out_cap = s->alt_cap;
     p.epoch = next_epoch(s);
-    e = crb::launch_replace(p, s->stream, nullptr);
+    e = p.nsub ? crb::launch_replace_super(p, s->stream, nullptr) : crb::launch_replace(p, s->stream, nullptr);
     if (e != cudaSuccess) return (int)e;
     ++s->launches;
     e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
@@ -413,7 +434,7 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
     s->q_n = n;
     s->q_params = p;
     s->kept_last = r.kept;
-    if (out_last) *out_last = r.kept ? r.last_kept : -1;
+    if (out_last) *out_last = r.kept ? last_kept_of(p, r) : -1;
     if (new_len) *new_len = s->len;
     return 0;
   }
@@ -431,8 +452,23 @@ int query_prefix64(Session* s, size_t limit, long long* kept, long long* last) {
     *last = (long long)lim - 1;
     return 0;
   }
-  const unsigned long long t = lim / crb::kTile, rel = lim % crb::kTile;
   cudaError_t e;
+  if (s->q_params.nsub) {
+    ReplaceParams p = s->q_params;
+    p.in = s->alt;  // the input of the last apply
+    p.query_limit64 = lim;
+    e = crb::launch_query_super(p, s->stream);
+    if (e != cudaSuccess) return (int)e;
+    ++s->launches;
+    e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return (int)e;
+    if (s->res_host->error_epoch == p.epoch) return kErrUnknown;
+    *kept = (long long)s->res_host->q_kept;
+    *last = s->res_host->q_last;
+    return 0;
+  }
+  const unsigned long long t = lim / crb::kTile, rel = lim % crb::kTile;
   if (rel == 0) {
     TileIncl ti;
     e = cudaMemcpyAsync(&ti, s->incl + (t - 1), sizeof(TileIncl), cudaMemcpyDeviceToHost, s->stream);
@@ -648,11 +684,14 @@ CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size
   memset(&p, 0, sizeof(p));
   crb::prepare_pattern_fields(p, pat, L);
   p.R = R;
-  const size_t tiles = (n + crb::kTile - 1) / crb::kTile;
+  p.nsub = crb::super_nsub(p.mode, L);
+  const size_t tile_bytes = (size_t)crb::kTile * (p.nsub ? p.nsub : 1u);
+  const size_t tiles = (n + tile_bytes - 1) / tile_bytes;
   if (tiles > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;
   p.num_tiles = (uint32_t)tiles;
   cudaError_t e = ensure_scratch(s, tiles, p.agg_entries);
   if (e != cudaSuccess) return (int)e;
+  p.tile_last = s->tile_last;
   memcpy(p.pat, pat, L);
   if (R) memcpy(p.rep, rep, R);
   p.in = d_in;
@@ -665,7 +704,7 @@ CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size
   p.res = s->res;
   p.epoch = next_epoch(s);
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
-  e = crb::launch_replace(p, st, nullptr);
+  e = p.nsub ? crb::launch_replace_super(p, st, nullptr) : crb::launch_replace(p, st, nullptr);
   if (e != cudaSuccess) return (int)e;
   ++s->launches;
   s->async_stream = st;

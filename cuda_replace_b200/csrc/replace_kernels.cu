@@ -25,6 +25,7 @@
 #include "replace_kernels.h"
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <mutex>
 
@@ -840,6 +841,943 @@ __global__ void empty_pattern_kernel(const uint8_t* __restrict__ in, unsigned lo
   }
 }
 
+// ============================================================================ super-tile kernel
+// One look-back per super-tile of nsub 16 KiB sub-tiles. Pass A streams the sub-tiles in
+// from HBM, keeps their candidate masks in shared memory and composes the super-tile's
+// carry function; after the look-back, pass B streams the same sub-tiles again (they are
+// still in L2) and writes the output. Loads run kNBuf ahead through a ring of buffers.
+namespace {
+
+constexpr int kNBuf = 2;
+constexpr int kMaxSub = 8;
+
+struct LayoutS {
+  uint32_t in0, outb, masks, pat, rep, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
+  uint32_t rs, inbytes;
+  uint32_t stage_bytes;  // output bytes the padded staging buffer holds
+};
+
+// Output bytes one 16 KiB sub-tile can produce, capped at three times its input.
+__host__ __device__ __forceinline__ uint32_t stage_ratio(uint32_t L, uint32_t R) {
+  if (L == 0 || R <= L) return 1;
+  const uint32_t r = (R + L - 1) / L;
+  return r < 3 ? r : 3;
+}
+
+__host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_t L, uint32_t R, uint32_t nsub) {
+  LayoutS s{};
+  uint32_t off = 0;
+  s.inbytes = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16) + 32;
+  s.in0 = off;
+  off += kNBuf * s.inbytes;
+  s.stage_bytes = kTile * stage_ratio(L, R) + 64;
+  s.outb = off;
+  off += align_up_u32((s.stage_bytes / 4 + s.stage_bytes / 128 + 2) * 4, 16);
+  s.masks = off;
+  off += nsub * kThreads * 8;
+  s.pat = off;
+  off += align_up_u32(L ? L : 1, 16);
+  s.rep = off;
+  off += align_up_u32(R + 16, 16);
+  if (mode == kModeSmall) {
+    s.rs = L | 1u;
+    s.segtab = off;
+    off += align_up_u32(kThreads * s.rs * 2, 16);
+    s.srec = off;
+    off += align_up_u32(nsub * kThreads * L, 16);
+    s.wtab = off;
+    off += align_up_u32(kWarps * L * 4, 16);
+    s.wrec = off;
+    off += align_up_u32(nsub * kWarps * L, 16);
+    s.subrec = off;
+    off += align_up_u32(nsub * L, 16);
+  }
+  s.total = off;
+  return s;
+}
+
+// Segment function as 16-bit entries (kept count in the low byte, carry-out in the high
+// byte) over carries [0, L), L <= 32.
+__device__ __forceinline__ void build_seg_table16(uint64_t mask, uint32_t L, uint32_t inv_l, uint64_t stride,
+                                                  uint16_t* row) {
+  uint32_t c = 0;
+  while (c < L) {
+    const uint64_t m = mask >> c;
+    if (m == 0) {
+      for (; c < L; ++c) row[c] = 0;
+      break;
+    }
+    const uint32_t e = c + (uint32_t)(__ffsll((long long)m) - 1);
+    const Walk w = seg_walk(mask, e, L, inv_l, stride);
+    const uint32_t carry = w.end > 64 ? w.end - 64 : 0;
+    const uint16_t v = (uint16_t)(w.cnt | (carry << 8));
+    const uint32_t hi = min(e + 1, L);
+    for (; c < hi; ++c) row[c] = v;
+  }
+}
+
+// The 17 words (68 bytes) starting at this thread's 64-byte segment; the 17th word is the
+// next lane's first word (read from shared memory only by the last lane of each warp), so
+// no load has lanes 64 bytes apart on the same bank.
+__device__ __forceinline__ void load_seg_words(const uint8_t* s, uint32_t w[17]) {
+  const uint4* v = reinterpret_cast<const uint4*>(s);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint4 q = v[i];
+    w[4 * i + 0] = q.x;
+    w[4 * i + 1] = q.y;
+    w[4 * i + 2] = q.z;
+    w[4 * i + 3] = q.w;
+  }
+  const uint32_t nxt = __shfl_down_sync(0xffffffffu, w[0], 1);
+  w[16] = ((threadIdx.x & 31u) == 31u) ? *reinterpret_cast<const uint32_t*>(s + 64) : nxt;
+}
+
+__device__ __forceinline__ uint64_t candidates_from_words(const uint32_t w[17], uint32_t p4, uint32_t m4) {
+  uint32_t lo = 0, hi = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t x = (j == 0) ? w[i] : __funnelshift_r(w[i], w[i + 1], 8 * j);
+      const uint32_t hit = (((x ^ p4) & m4) == 0u) ? 1u : 0u;
+      const int pos = 4 * i + j;
+      if (pos < 32)
+        lo |= hit << pos;
+      else
+        hi |= hit << (pos - 32);
+    }
+  }
+  return ((uint64_t)hi << 32) | lo;
+}
+
+// Output staging: a word buffer with one padding word after every 32, so threads that
+// write their (contiguous) outputs word by word land on different banks.
+__device__ __forceinline__ uint32_t stg_pad(uint32_t w) { return w + (w >> 5); }
+
+// 4 bytes at an arbitrary shared-memory byte address (two aligned loads and a funnel shift).
+__device__ __forceinline__ uint32_t ld_u32_unaligned(const uint8_t* p) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = (uint32_t)(a & 3u) * 8u;
+  return sh ? __funnelshift_r(q[0], q[1], sh) : q[0];
+}
+
+// Streams one thread's output bytes into the staging buffer: whole words are stored as
+// words; the partial first and last words (shared with the neighbouring threads) byte by byte.
+struct Emitter {
+  uint32_t* stg;
+  unsigned long long acc;
+  uint32_t nb;    // bytes held in acc (the first `skip` of them belong to the previous thread)
+  uint32_t wpos;  // staging word of acc's first byte
+  uint32_t skip;
+
+  __device__ __forceinline__ void init(uint32_t* s, uint32_t start_byte) {
+    stg = s;
+    acc = 0;
+    nb = start_byte & 3u;
+    wpos = start_byte >> 2;
+    skip = nb;
+  }
+  __device__ __forceinline__ void store_bytes(uint32_t word, uint32_t from, uint32_t to) {
+    uint8_t* b = reinterpret_cast<uint8_t*>(stg + stg_pad(wpos));
+    for (uint32_t i = from; i < to; ++i) b[i] = (uint8_t)(word >> (8 * i));
+  }
+  __device__ __forceinline__ void put_word(uint32_t word) {
+    if (skip) {
+      store_bytes(word, skip, 4);
+      skip = 0;
+    } else {
+      stg[stg_pad(wpos)] = word;
+    }
+  }
+  // append k (1..4) bytes held in the low bytes of v
+  __device__ __forceinline__ void append(uint32_t v, uint32_t k) {
+    acc |= (unsigned long long)(k == 4 ? v : (v & ((1u << (8 * k)) - 1u))) << (8 * nb);
+    nb += k;
+    if (nb >= 4) {
+      put_word((uint32_t)acc);
+      acc >>= 32;
+      nb -= 4;
+      ++wpos;
+    }
+  }
+  __device__ __forceinline__ void finish() {
+    if (nb > skip) store_bytes((uint32_t)acc, skip, nb);
+  }
+};
+
+// Literal bytes src[0, len) from shared memory.
+__device__ __forceinline__ void emit_literal(Emitter& e, const uint8_t* src, uint32_t len) {
+  uint32_t i = 0;
+  for (; i + 4 <= len; i += 4) e.append(ld_u32_unaligned(src + i), 4);
+  for (; i < len; ++i) e.append(src[i], 1);
+}
+
+// r copies of the replacement: rrep holds the replacement repeated (at least R + 8 bytes);
+// step4 = 4 mod R.
+__device__ __forceinline__ void emit_repeat(Emitter& e, const uint8_t* rrep, uint32_t R, uint32_t step4,
+                                            uint32_t r) {
+  uint32_t total = r * R, ph = 0;
+  for (; total >= 4; total -= 4) {
+    e.append(ld_u32_unaligned(rrep + ph), 4);
+    ph += step4;
+    if (ph >= R) ph -= R;
+  }
+  for (; total; --total) {
+    e.append(rrep[ph], 1);
+    if (++ph == R) ph = 0;
+  }
+}
+
+// Warp-level bounded wait over the window of predecessors j = base - lane (j < 0 is the
+// virtual tile before tile 0, treated as inclusive with K = 0, carry = 0). Returns the lane
+// of the nearest inclusive tile (32 if none) once every nearer lane has at least its
+// aggregate, or -1 when the wait gave up. *st receives this lane's state.
+__device__ __forceinline__ int warp_wait_window(const ReplaceParams& p, long long base, uint32_t* st) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const long long j = base - (long long)lane;
+  const uint32_t want = p.epoch << 2;
+  unsigned long long t0 = 0;
+  uint32_t ns = 32;
+  for (;;) {
+    uint32_t s = 0;
+    if (j < 0) {
+      s = kStInc;
+    } else {
+      const uint32_t v = ld_acquire_u32(p.status + j);
+      if ((v & ~3u) == want) s = v & 3u;
+    }
+    const uint32_t ready = __ballot_sync(0xffffffffu, s != 0);
+    const uint32_t incm = __ballot_sync(0xffffffffu, s == kStInc);
+    const uint32_t pl = incm ? (uint32_t)(__ffs(incm) - 1) : 32u;
+    const uint32_t need = pl == 32u ? 0xffffffffu : ((1u << pl) - 1u);
+    if ((ready & need) == need) {
+      *st = s;
+      return (int)pl;
+    }
+    if (aborted(p)) return -1;
+    const unsigned long long now = global_ns();
+    if (t0 == 0) {
+      t0 = now;
+    } else if (now - t0 > kSpinLimitNs) {
+      if (lane == 0) set_error(p);
+      return -1;
+    }
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+  }
+}
+
+// Mode free: a block's function is carry_out(c) = max(c - span, cover), count constant.
+// Look-back over super-tiles of S bytes by warp 0; returns (K, carry) for tile t.
+__device__ __forceinline__ bool lookback_free(const ReplaceParams& p, uint32_t t, unsigned long long S,
+                                              unsigned long long* K_out, uint32_t* c_out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long acc_cnt = 0;
+  long long acc_cover = 0;
+  unsigned long long acc_span = 0;
+  long long base = (long long)t - 1;
+  for (;;) {
+    const long long j = base - (long long)lane;
+    uint32_t st;
+    const int plr = warp_wait_window(p, base, &st);
+    if (plr < 0) return false;
+    const uint32_t pl = (uint32_t)plr;
+    unsigned long long cnt = 0;
+    long long val = LLONG_MIN / 4;
+    if (lane < pl) {
+      const unsigned long long e = __ldcg(p.agg + j);
+      cnt = e & 0xFFFFFFFFull;
+      val = (long long)(e >> 32) - (long long)(lane * S);
+    } else if (lane == pl) {
+      if (j >= 0) {
+        cnt = __ldcg(&p.incl[j].kept);
+        val = (long long)__ldcg(&p.incl[j].carry) - (long long)(lane * S);
+      } else {
+        val = 0;
+      }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+      cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+      const long long o = __shfl_xor_sync(0xffffffffu, val, d);
+      val = o > val ? o : val;
+    }
+    if (pl < 32) {
+      const long long c1 = val - (long long)acc_span;
+      const long long c = c1 > acc_cover ? c1 : acc_cover;
+      *K_out = cnt + acc_cnt;
+      *c_out = c > 0 ? (uint32_t)c : 0u;
+      return true;
+    }
+    const long long cov = val - (long long)acc_span;
+    acc_cover = cov > acc_cover ? cov : acc_cover;
+    acc_cnt += cnt;
+    acc_span += 32ull * S;
+    base -= 32;
+  }
+}
+
+// Mode small (L <= 32): tile functions are tables over carries; lane c holds entry c.
+// acc is the function of the tiles between the current window and t.
+__device__ __forceinline__ bool lookback_small(const ReplaceParams& p, uint32_t t, uint32_t L,
+                                               unsigned long long* K_out, uint32_t* c_out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long acc_cnt = 0;
+  uint32_t acc_carry = lane;
+  long long base = (long long)t - 1;
+  for (;;) {
+    uint32_t st;
+    const int plr = warp_wait_window(p, base, &st);
+    if (plr < 0) return false;
+    const uint32_t pl = (uint32_t)plr;
+    uint32_t e[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      e[i] = 0;
+      if ((uint32_t)i < pl && lane < L) {
+        const unsigned long long v = __ldcg(p.agg + (unsigned long long)(base - i) * L + lane);
+        e[i] = (uint32_t)(v & 0x00FFFFFFull) | ((uint32_t)(v >> 32) << 24);
+      }
+    }
+    if (pl < 32) {
+      unsigned long long K = 0;
+      uint32_t x = 0;
+      const long long jp = base - (long long)pl;
+      if (jp >= 0) {
+        K = __ldcg(&p.incl[jp].kept);
+        x = __ldcg(&p.incl[jp].carry);
+      }
+#pragma unroll
+      for (int i = 31; i >= 0; --i) {
+        if ((uint32_t)i < pl) {
+          const uint32_t v = __shfl_sync(0xffffffffu, e[i], x);
+          K += v & 0x00FFFFFFu;
+          x = v >> 24;
+        }
+      }
+      *K_out = K + __shfl_sync(0xffffffffu, acc_cnt, x);
+      *c_out = __shfl_sync(0xffffffffu, acc_carry, x);
+      return true;
+    }
+    // the whole window holds aggregates: compose it and put it in front of acc
+    uint32_t y = lane < L ? lane : 0u;
+    unsigned long long wc = 0;
+#pragma unroll
+    for (int i = 31; i >= 0; --i) {
+      const uint32_t v = __shfl_sync(0xffffffffu, e[i], y);
+      wc += v & 0x00FFFFFFu;
+      y = v >> 24;
+    }
+    const unsigned long long ac = __shfl_sync(0xffffffffu, acc_cnt, y);
+    const uint32_t ax = __shfl_sync(0xffffffffu, acc_carry, y);
+    acc_cnt = wc + ac;
+    acc_carry = ax;
+    base -= 32;
+  }
+}
+
+}  // namespace
+
+// Number of 16 KiB sub-tiles in super-tile `tile`.
+__device__ __forceinline__ uint32_t subs_in_tile(uint32_t tile, unsigned long long S, unsigned long long n,
+                                                 uint32_t nsub) {
+  const unsigned long long rem = n - (unsigned long long)tile * S;
+  const unsigned long long m = (rem + kTile - 1) / kTile;
+  return m < nsub ? (uint32_t)m : nsub;
+}
+
+// Ring of kNBuf shared-memory buffers fed by 1-D TMA loads. Every thread keeps the same
+// `consumed` count; only thread 0 issues (and tracks the issue position).
+struct LoadRing {
+  uint32_t issued, consumed;
+  uint32_t iq, iph, ij;  // next load: queue slot (0 current, 1 next super-tile), pass, sub-tile
+
+  __device__ __forceinline__ void init() {
+    issued = consumed = 0;
+    iq = iph = ij = 0;
+  }
+  __device__ __forceinline__ void issue(const ReplaceParams& p, uint8_t* smem, const LayoutS& lay,
+                                        uint64_t* bars, uint32_t* q, unsigned long long S,
+                                        unsigned long long n16, uint32_t want_a) {
+    const uint32_t NT = p.num_tiles;
+    while (issued - consumed < (uint32_t)kNBuf) {
+      if (iq >= 2) break;
+      if (iq == 1 && q[1] == 0xFFFFFFFFu) {
+        const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
+        q[1] = nx < NT ? nx : NT;
+      }
+      const uint32_t tile = q[iq];
+      if (tile >= NT) break;
+      const uint32_t m = subs_in_tile(tile, S, p.n, p.nsub);
+      const unsigned long long start = (unsigned long long)tile * S + (unsigned long long)ij * kTile;
+      const unsigned long long avail = n16 - start;
+      const uint32_t want = iph == 0 ? want_a : (uint32_t)kTile;
+      const uint32_t bytes = avail < want ? (uint32_t)avail : want;
+      const uint32_t b = issued % kNBuf;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&bars[b], bytes);
+      bulk_load(smem + lay.in0 + b * lay.inbytes, p.in + start, bytes, &bars[b]);
+      ++issued;
+      if (++ij == m) {
+        ij = 0;
+        if (iph == 0) {
+          iph = 1;
+        } else {
+          iph = 0;
+          ++iq;
+        }
+      }
+    }
+  }
+  // Wait for the next load in consumption order; returns its buffer.
+  __device__ __forceinline__ uint8_t* wait(const ReplaceParams& p, uint8_t* smem, const LayoutS& lay,
+                                           uint64_t* bars, uint32_t* fail) {
+    const uint32_t b = consumed % kNBuf;
+    const uint32_t parity = (consumed / kNBuf) & 1u;
+    if (!wait_tile(&bars[b], parity)) {
+      if (threadIdx.x == 0) {
+        set_error(p);
+        *fail = 1;
+      }
+    }
+    return smem + lay.in0 + b * lay.inbytes;
+  }
+  __device__ __forceinline__ void release() { ++consumed; }
+  __device__ __forceinline__ void shift() { iq = iq > 0 ? iq - 1 : 0; }
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid_constant__ ReplaceParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t s_bar[kNBuf];
+  __shared__ uint32_t s_scan[kWarps];
+  __shared__ uint32_t s_q[2];  // current and next super-tile of this CTA
+  __shared__ unsigned long long s_kexcl;
+  __shared__ uint32_t s_cin;
+  __shared__ uint32_t s_fail;
+  __shared__ uint32_t s_sub_lco[kMaxSub];
+
+  const uint32_t L = p.L, R = p.R, nsub = p.nsub;
+  const LayoutS lay = make_layout_s(MODE, L, R, nsub);
+  uint8_t* ps = smem + lay.pat;
+  uint8_t* rs = smem + lay.rep;
+  uint8_t* ob = smem + lay.outb;
+  uint64_t* masks = reinterpret_cast<uint64_t*>(smem + lay.masks);
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t sb = tid * kSeg;
+  const unsigned long long n = p.n;
+  const unsigned long long n16 = (n + 15ull) & ~15ull;
+  const unsigned long long S = (unsigned long long)nsub * kTile;
+  const uint32_t want_a = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16);
+  const uint32_t NT = p.num_tiles;
+
+  {
+    const uint8_t* psrc = L <= (uint32_t)kInlineMax ? p.pat : p.pat_ext;
+    const uint8_t* rsrc = R <= (uint32_t)kInlineMax ? p.rep : p.rep_ext;
+    for (uint32_t i = tid; i < L; i += kThreads) ps[i] = psrc[i];
+    // the replacement repeated: rs[i] = rep[i mod R] for i < R + 16
+    for (uint32_t i = tid; i < R + 16; i += kThreads) rs[i] = R ? rsrc[i % R] : (uint8_t)0;
+  }
+  const uint32_t step4 = R ? 4u % R : 0u;
+
+  // ---- load ring: thread 0 issues loads in the order they will be consumed:
+  // for each super-tile of this CTA, pass A (sub-tile + halo) then pass B (sub-tile).
+  LoadRing ring;
+  ring.init();
+  if (tid == 0) {
+    for (int b = 0; b < kNBuf; ++b) mbar_init(&s_bar[b], 1);
+    fence_mbar_init();
+    const uint32_t first = atomicAdd(&p.res->tile_counter, 1u);
+    s_q[0] = first < NT ? first : NT;
+    s_q[1] = 0xFFFFFFFFu;
+    s_fail = 0;
+  }
+  __syncthreads();
+  if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+
+  for (;;) {
+    __syncthreads();
+    const uint32_t t = s_q[0];
+    if (t >= NT) break;
+    const uint32_t m = subs_in_tile(t, S, n, nsub);
+    const unsigned long long tstart = (unsigned long long)t * S;
+
+    // ================= pass A: candidates and the super-tile function
+    uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 0, lane = carry
+    unsigned long long fr_cnt = 0;           // kModeFree: thread 0
+    long long fr_lco = 0;
+    for (uint32_t j = 0; j < m; ++j) {
+      uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
+      const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
+      uint32_t W[17];
+      load_seg_words(tb + sb, W);
+      uint64_t mask = candidates_from_words(W, p.p4, p.m4);
+      {
+        uint32_t lo = 0, hi = 0;
+        if (p.block_before > gseg) {
+          const unsigned long long d = p.block_before - gseg;
+          lo = d < 64ull ? (uint32_t)d : 64u;
+        }
+        if (n >= L && n - L + 1 > gseg) {
+          const unsigned long long d = n - L + 1 - gseg;
+          hi = d < 64ull ? (uint32_t)d : 64u;
+        }
+        mask &= low_bits(hi) & ~low_bits(lo);
+      }
+      if (L > 4) mask = verify_tail(mask, tb + sb, ps, L);
+      masks[j * kThreads + tid] = mask;
+      if (MODE == kModeFree) {
+        const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
+        const uint32_t cend = mask ? sb + last + L : 0u;
+        uint32_t tot_cend, tot_cnt;
+        (void)block_excl_scan(cend, 0u, OpMax(), s_scan, &tot_cend);
+        (void)block_excl_scan((uint32_t)__popcll(mask), 0u, OpSum(), s_scan, &tot_cnt);
+        if (tid == 0) {
+          const long long lco = tot_cend > (uint32_t)kTile ? (long long)(tot_cend - kTile) : 0ll;
+          s_sub_lco[j] = (uint32_t)lco;
+          const long long shifted = fr_lco - (long long)kTile;
+          fr_lco = shifted > lco ? shifted : lco;
+          fr_cnt += tot_cnt;
+        }
+      } else {
+        uint16_t* segtab = reinterpret_cast<uint16_t*>(smem + lay.segtab);
+        build_seg_table16(mask, L, p.inv_l, p.stride_mask, segtab + tid * lay.rs);
+        __syncthreads();
+        uint8_t* srec = smem + lay.srec + (size_t)j * kThreads * L;
+        uint32_t* wtab = reinterpret_cast<uint32_t*>(smem + lay.wtab);
+        if (lane < L) {
+          uint32_t x = lane, cnt = 0;
+          const uint32_t seg0 = warp * 32u;
+#pragma unroll 8
+          for (uint32_t k = 0; k < 32; ++k) {
+            const uint32_t seg = seg0 + k;
+            srec[seg * L + lane] = (uint8_t)x;
+            const uint32_t v = segtab[seg * lay.rs + x];
+            cnt += v & 0xFFu;
+            x = v >> 8;
+          }
+          wtab[warp * L + lane] = cnt | (x << 16);
+        }
+        __syncthreads();
+        if (warp == 0) {
+          uint8_t* wrec = smem + lay.wrec + (size_t)j * kWarps * L;
+          uint32_t y = lane < L ? lane : 0u, cnt = 0;
+#pragma unroll
+          for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
+            if (lane < L) wrec[w * L + lane] = (uint8_t)y;
+            const uint32_t v = wtab[w * L + y];
+            cnt += v & 0xFFFFu;
+            y = v >> 16;
+          }
+          // compose the sub-tile function into the super-tile function
+          if (lane < L) (smem + lay.subrec)[j * L + lane] = (uint8_t)sup_carry;
+          const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
+          const uint32_t tx = __shfl_sync(0xffffffffu, y, sup_carry);
+          sup_cnt += tc;
+          sup_carry = tx;
+        }
+      }
+      __syncthreads();
+      ring.release();
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+    }
+
+    // ================= publish the aggregate, look back, publish the inclusive prefix
+    if (MODE == kModeFree) {
+      if (tid == 0) {
+        if (t > 0) {
+          __stcg(p.agg + t, fr_cnt | ((unsigned long long)fr_lco << 32));
+          __threadfence();
+          st_release_u32(p.status + t, (p.epoch << 2) | kStAgg);
+        }
+      }
+    } else {
+      if (warp == 0) {
+        if (t > 0 && lane < L)
+          __stcg(p.agg + (unsigned long long)t * L + lane, (unsigned long long)sup_cnt |
+                                                                ((unsigned long long)sup_carry << 32));
+        __threadfence();
+        __syncwarp();
+        if (t > 0 && lane == 0) st_release_u32(p.status + t, (p.epoch << 2) | kStAgg);
+      }
+    }
+    if (warp == 0) {
+      unsigned long long K = 0;
+      uint32_t c = 0;
+      bool ok = true;
+      if (t > 0) ok = MODE == kModeFree ? lookback_free(p, t, S, &K, &c) : lookback_small(p, t, L, &K, &c);
+      if (!ok) {
+        K = 0;
+        c = 0;
+        if (lane == 0) s_fail = 1;
+      }
+      // own inclusive prefix
+      unsigned long long Kin;
+      uint32_t cout;
+      if (MODE == kModeFree) {
+        const unsigned long long fcnt = __shfl_sync(0xffffffffu, fr_cnt, 0);
+        const long long flco = __shfl_sync(0xffffffffu, fr_lco, 0);
+        const long long sh = (long long)c - (long long)S;
+        const long long co = sh > flco ? sh : flco;
+        Kin = K + fcnt;
+        cout = co > 0 ? (uint32_t)co : 0u;
+      } else {
+        Kin = K + __shfl_sync(0xffffffffu, sup_cnt, c);
+        cout = __shfl_sync(0xffffffffu, sup_carry, c);
+      }
+      if (lane == 0) {
+        __stcg(&p.incl[t].kept, Kin);
+        __stcg(&p.incl[t].carry, cout);
+        __threadfence();
+        st_release_u32(p.status + t, (p.epoch << 2) | kStInc);
+        s_kexcl = K;
+        s_cin = c;
+      }
+    }
+    __syncthreads();
+    const uint32_t cin = s_cin;
+    const unsigned long long kexcl = s_kexcl;
+    const long long delta = (long long)R - (long long)L;
+    unsigned long long O = (unsigned long long)((long long)(tstart + cin) + (long long)kexcl * delta);
+    const bool failed = s_fail != 0;
+
+    // ================= pass B: exact kept starts and output
+    uint32_t csub = cin;        // kModeFree: carry into sub-tile j
+    long long last_abs = -1;    // last kept start seen by this thread
+    for (uint32_t j = 0; j < m; ++j) {
+      uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
+      const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
+      const unsigned long long gseg = sstart + sb;
+      const uint64_t mask = masks[j * kThreads + tid];
+      uint32_t x_in;
+      uint64_t kept;
+      uint32_t cnt;
+      if (MODE == kModeFree) {
+        const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
+        const uint32_t cend = mask ? sb + last + L : 0u;
+        uint32_t tot;
+        const uint32_t pre = block_excl_scan(cend, 0u, OpMax(), s_scan, &tot);
+        const uint32_t cov = csub > pre ? csub : pre;
+        x_in = cov > sb ? cov - sb : 0u;
+        kept = mask;
+        cnt = (uint32_t)__popcll(mask);
+        const long long sh = (long long)csub - (long long)kTile;
+        const long long lco = (long long)s_sub_lco[j];
+        const long long nx = sh > lco ? sh : lco;
+        csub = nx > 0 ? (uint32_t)nx : 0u;
+      } else {
+        const uint32_t cs = (smem + lay.subrec)[j * L + cin];
+        const uint32_t cw = (smem + lay.wrec)[((size_t)j * kWarps + warp) * L + cs];
+        x_in = (smem + lay.srec)[((size_t)j * kThreads + tid) * L + cw];
+        if (x_in >= 64u) {
+          kept = 0;
+          cnt = 0;
+        } else {
+          const Walk w = seg_walk(mask, x_in, L, p.inv_l, p.stride_mask);
+          kept = w.kept;
+          cnt = w.cnt;
+        }
+      }
+      const uint32_t V = gseg >= n ? 0u : ((n - gseg) < 64ull ? (uint32_t)(n - gseg) : 64u);
+      uint32_t covered = x_in < V ? x_in : V;
+      if (cnt) {
+        const uint32_t lastk = 63u - (uint32_t)__clzll((long long)kept);
+        const uint32_t over = (lastk + L > V) ? lastk + L - V : 0u;
+        covered += cnt * L - over;
+        last_abs = (long long)(gseg + lastk);
+      }
+      const uint32_t olen = V - covered + cnt * R;
+      uint32_t sub_olen;
+      const uint32_t ooff = block_excl_scan(olen, 0u, OpSum(), s_scan, &sub_olen);
+      const bool fits = (O + sub_olen <= p.out_cap) && (O <= p.out_cap);
+      if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
+      uint32_t W[17];
+      load_seg_words(tb + sb, W);
+      const uint32_t sh = (uint32_t)(O & 15ull);
+      if (fits && !failed && sh + sub_olen + 16u <= lay.stage_bytes) {
+        // ---- assemble this sub-tile's output in the padded staging buffer
+        uint32_t* stg = reinterpret_cast<uint32_t*>(ob);
+        uint8_t* sbytes = ob;
+        const uint32_t cur = sh + ooff;
+        if (olen && kept == 0 && x_in == 0 && V == 64u) {
+          // literal-only segment: its 64 input bytes, shifted to the output word grid
+          const uint32_t d = (4u - (cur & 3u)) & 3u;
+          for (uint32_t i = 0; i < d; ++i) {
+            const uint32_t b = cur + i;
+            sbytes[stg_pad(b >> 2) * 4u + (b & 3u)] = (uint8_t)(W[0] >> (8u * i));
+          }
+          const uint32_t wb = (cur + d) >> 2;
+          if (d == 0) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) stg[stg_pad(wb + k)] = W[k];
+          } else {
+#pragma unroll
+            for (int k = 0; k < 15; ++k) stg[stg_pad(wb + k)] = __funnelshift_r(W[k], W[k + 1], 8u * d);
+            for (uint32_t i = d + 60u; i < 64u; ++i) {
+              const uint32_t b = cur + i;
+              sbytes[stg_pad(b >> 2) * 4u + (b & 3u)] = (uint8_t)(W[15] >> (8u * (i & 3u)));
+            }
+          }
+        } else if (olen) {
+          Emitter e;
+          e.init(stg, cur);
+          const uint8_t* src = tb + sb;
+          uint32_t pos = x_in < V ? x_in : V;
+          while (pos < V) {
+            const uint64_t km = pos < 64u ? (kept >> pos) : 0ull;
+            uint32_t nk = km ? pos + (uint32_t)(__ffsll((long long)km) - 1) : V;
+            if (nk > V) nk = V;
+            if (nk > pos) emit_literal(e, src + pos, nk - pos);
+            if (nk >= V) break;
+            uint32_t r = 1;  // kept starts nk, nk+L, ... with nothing literal between them
+            if (L < 64u) {
+              const uint64_t holes = p.stride_mask & ~(kept >> nk);
+              const uint32_t h = holes ? (uint32_t)(__ffsll((long long)holes) - 1) : 64u;
+              r = ((h + L - 1) * p.inv_l) >> 16;
+            }
+            if (R) emit_repeat(e, rs, R, step4, r);
+            pos = nk + r * L;
+          }
+          e.finish();
+        }
+        __syncthreads();
+        // ---- copy out: coalesced 16-byte stores; partial chunks at both ends byte by byte
+        const unsigned long long base_g = O - sh;
+        const uint32_t total = sh + sub_olen;
+        const uint32_t nch = (total + 15u) >> 4;
+        for (uint32_t c = tid; c < nch; c += kThreads) {
+          const uint32_t lo = c << 4, hi = lo + 16u;
+          if (lo >= sh && hi <= total) {
+            const uint32_t w = c << 2;
+            uint4 v;
+            v.x = stg[stg_pad(w)];
+            v.y = stg[stg_pad(w + 1)];
+            v.z = stg[stg_pad(w + 2)];
+            v.w = stg[stg_pad(w + 3)];
+            *reinterpret_cast<uint4*>(p.out + base_g + lo) = v;
+          } else {
+            const uint32_t b0 = lo > sh ? lo : sh, b1 = hi < total ? hi : total;
+            for (uint32_t b = b0; b < b1; ++b) p.out[base_g + b] = sbytes[stg_pad(b >> 2) * 4u + (b & 3u)];
+          }
+        }
+      } else if (fits && !failed) {
+        // very large expansions: windows of the output, byte by byte
+        for (uint32_t w0 = 0; w0 < sub_olen; w0 += kOutWin) {
+          const uint32_t w1 = (w0 + kOutWin) < sub_olen ? (w0 + kOutWin) : sub_olen;
+          const unsigned long long g0 = O + w0;
+          const uint32_t sh = (uint32_t)(g0 & 15ull);
+          uint8_t* obw = ob + sh;
+          if (olen && ooff < w1 && ooff + olen > w0) {
+            const uint8_t* src = tb + sb;
+            uint32_t o = ooff;
+            uint32_t pos = x_in < V ? x_in : V;
+            while (pos < V) {
+              const uint64_t km = pos < 64u ? (kept >> pos) : 0ull;
+              uint32_t nk = km ? pos + (uint32_t)(__ffsll((long long)km) - 1) : V;
+              if (nk > V) nk = V;
+              copy_clip(obw, o, src + pos, nk - pos, w0, w1);
+              o += nk - pos;
+              if (nk >= V) break;
+              copy_clip(obw, o, rs, R, w0, w1);
+              o += R;
+              pos = nk + L;
+            }
+          }
+          fence_proxy_async_smem();
+          __syncthreads();
+          const unsigned long long gend = O + w1;
+          const unsigned long long a0 = (g0 + 15ull) & ~15ull;
+          const unsigned long long a1 = gend & ~15ull;
+          if (a1 > a0) {
+            if (tid == 0) {
+              bulk_store(p.out + a0, ob + sh + (uint32_t)(a0 - g0), (uint32_t)(a1 - a0));
+              bulk_commit();
+            }
+            if (tid < (uint32_t)(a0 - g0)) p.out[g0 + tid] = obw[tid];
+            if (tid >= 32u && tid - 32u < (uint32_t)(gend - a1))
+              p.out[a1 + (tid - 32u)] = obw[(uint32_t)(a1 - g0) + (tid - 32u)];
+          } else {
+            for (uint32_t i = tid; i < (uint32_t)(gend - g0); i += kThreads) p.out[g0 + i] = obw[i];
+          }
+          if (tid == 0) bulk_wait_read_all();
+          __syncthreads();
+        }
+      }
+      O += sub_olen;
+      __syncthreads();
+      ring.release();
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+    }
+
+    // ================= per-super-tile records: last kept start, totals
+    {
+      const uint32_t last1 = last_abs >= 0 ? (uint32_t)((unsigned long long)last_abs - tstart + 1) : 0u;
+      uint32_t tot_last1;
+      (void)block_excl_scan(last1, 0u, OpMax(), s_scan, &tot_last1);
+      if (tid == 0) {
+        const long long lastt = tot_last1 ? (long long)(tstart + tot_last1 - 1) : -1ll;
+        __stcg(p.tile_last + t, lastt);
+        if (lastt >= 0)
+          atomicMax(&p.res->last_tagged, ((unsigned long long)p.epoch << 40) | (unsigned long long)(lastt + 1));
+        if (t == NT - 1) {
+          p.res->out_len = O;
+          p.res->kept = __ldcg(&p.incl[t].kept);
+        }
+      }
+    }
+    // advance the queue
+    if (tid == 0) {
+      s_q[0] = s_q[1] == 0xFFFFFFFFu ? 0xFFFFFFFFu : s_q[1];
+      s_q[1] = 0xFFFFFFFFu;
+      if (s_q[0] == 0xFFFFFFFFu) {
+        const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
+        s_q[0] = nx < NT ? nx : NT;
+      }
+      ring.shift();
+      s_fail = 0;
+      ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+    }
+  }
+
+  if (tid == 0) {
+    bulk_wait_all();
+    __threadfence();
+    const unsigned int d = atomicAdd(&p.res->done_ctas, 1u);
+    if (d == gridDim.x - 1) {
+      atomicExch(&p.res->tile_counter, 0u);
+      atomicExch(&p.res->done_ctas, 0u);
+      __threadfence();
+    }
+  }
+}
+
+// One CTA answers query_prefix for a super-tile layout: kept starts before limit and the
+// last one, re-deriving the kept starts of the super-tile that holds limit from its exact
+// carry-in (the predecessor's inclusive prefix) and searching earlier super-tiles' records.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) query_super_kernel(const __grid_constant__ ReplaceParams p) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ uint32_t s_scan[kWarps];
+  __shared__ uint32_t s_x;
+  __shared__ unsigned long long s_k;
+  __shared__ long long s_last;
+  __shared__ uint32_t s_ok;
+  const uint32_t L = p.L;
+  const LayoutS lay = make_layout_s(kModeFree, L, p.R, 1);
+  uint8_t* tb = smem + lay.in0;
+  uint8_t* ps = smem + lay.pat;
+  uint64_t* masks = reinterpret_cast<uint64_t*>(smem + lay.masks);
+  const uint32_t tid = threadIdx.x, sb = tid * kSeg;
+  const unsigned long long n = p.n, n16 = (n + 15ull) & ~15ull;
+  const unsigned long long S = (unsigned long long)p.nsub * kTile;
+  const unsigned long long limit = p.query_limit64;
+  const uint32_t t = (uint32_t)(limit / S);
+  const unsigned long long rel = limit - (unsigned long long)t * S;
+  {
+    const uint8_t* psrc = L <= (uint32_t)kInlineMax ? p.pat : p.pat_ext;
+    for (uint32_t i = tid; i < L; i += kThreads) ps[i] = psrc[i];
+  }
+  if (tid == 0) {
+    mbar_init(&s_bar, 1);
+    fence_mbar_init();
+    s_ok = 1;
+    s_k = t > 0 ? __ldcg(&p.incl[t - 1].kept) : 0ull;
+    s_x = t > 0 ? __ldcg(&p.incl[t - 1].carry) : 0u;
+    s_last = -1;
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  for (uint32_t j = 0; (unsigned long long)j * kTile < rel; ++j) {
+    const unsigned long long sstart = (unsigned long long)t * S + (unsigned long long)j * kTile;
+    if (tid == 0) {
+      const uint32_t want = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16);
+      const unsigned long long avail = n16 - sstart;
+      const uint32_t bytes = avail < want ? (uint32_t)avail : want;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&s_bar, bytes);
+      bulk_load(tb, p.in + sstart, bytes, &s_bar);
+    }
+    if (!wait_tile(&s_bar, phase) && tid == 0) s_ok = 0;
+    phase ^= 1u;
+    const unsigned long long gseg = sstart + sb;
+    uint64_t mask = seg_candidates4(tb + sb, p.p4, p.m4);
+    {
+      uint32_t lo = 0, hi = 0;
+      if (p.block_before > gseg) {
+        const unsigned long long d = p.block_before - gseg;
+        lo = d < 64ull ? (uint32_t)d : 64u;
+      }
+      if (n >= L && n - L + 1 > gseg) {
+        const unsigned long long d = n - L + 1 - gseg;
+        hi = d < 64ull ? (uint32_t)d : 64u;
+      }
+      mask &= low_bits(hi) & ~low_bits(lo);
+    }
+    if (L > 4) mask = verify_tail(mask, tb + sb, ps, L);
+    masks[tid] = mask;
+    __syncthreads();
+    if (tid == 0) {
+      const unsigned long long lim = rel - (unsigned long long)j * kTile;  // limit relative to this sub-tile
+      uint32_t x = s_x;
+      unsigned long long K = s_k;
+      long long last = s_last;
+      for (uint32_t seg = 0; seg < (uint32_t)kThreads; ++seg) {
+        const unsigned long long base = (unsigned long long)seg * 64u;
+        uint64_t kept;
+        uint32_t xn;
+        if (MODE == kModeFree) {
+          kept = masks[seg];
+          xn = 0;
+        } else if (x >= 64u) {
+          kept = 0;
+          xn = x - 64u;
+        } else {
+          const Walk w = seg_walk(masks[seg], x, L, p.inv_l, p.stride_mask);
+          kept = w.kept;
+          xn = w.end > 64u ? w.end - 64u : 0u;
+        }
+        if (base < lim) {
+          const uint64_t kb = kept & low_bits(lim - base < 64ull ? (uint32_t)(lim - base) : 64u);
+          K += (unsigned long long)__popcll(kb);
+          if (kb) last = (long long)(sstart + base + 63u - (uint32_t)__clzll((long long)kb));
+        }
+        x = xn;
+      }
+      s_x = x;
+      s_k = K;
+      s_last = last;
+    }
+    __syncthreads();
+  }
+  // last kept start in earlier super-tiles when none was found in this one
+  uint32_t best_hi = 0, best_lo = 0;
+  if (s_last < 0) {
+    for (uint32_t i = tid; i < t; i += kThreads) {
+      const long long v = __ldcg(p.tile_last + i);
+      const unsigned long long u = (unsigned long long)(v + 1);
+      const uint32_t hi = (uint32_t)(u >> 32), lo = (uint32_t)u;
+      if (hi > best_hi || (hi == best_hi && lo > best_lo)) {
+        best_hi = hi;
+        best_lo = lo;
+      }
+    }
+  }
+  uint32_t tot_hi;
+  (void)block_excl_scan(best_hi, 0u, OpMax(), s_scan, &tot_hi);
+  uint32_t tot_lo;
+  (void)block_excl_scan(best_hi == tot_hi ? best_lo : 0u, 0u, OpMax(), s_scan, &tot_lo);
+  if (tid == 0) {
+    long long last = s_last;
+    if (last < 0) last = (long long)(((unsigned long long)tot_hi << 32) | tot_lo) - 1;
+    p.res->q_kept = s_k;
+    p.res->q_last = last;
+    if (!s_ok) set_error(p);
+  }
+}
+
 // ============================================================================ host side
 namespace {
 
@@ -928,6 +1866,63 @@ void prepare_pattern_fields(ReplaceParams& p, const uint8_t* pat, uint32_t L) {
 }
 
 uint32_t tile_kernel_smem_bytes(uint32_t mode, uint32_t L, uint32_t R) { return make_layout(mode, L, R).total; }
+uint32_t super_nsub(uint32_t mode, uint32_t L) {
+  if (mode == kModeFree) return kMaxSub;
+  if (mode == kModeSmall && L >= 2 && L <= 32) {
+    const uint32_t by_rec = 128u / L;  // keep the per-segment carry records within 32 KiB
+    return by_rec < (uint32_t)kMaxSub ? (by_rec ? by_rec : 1u) : (uint32_t)kMaxSub;
+  }
+  return 0;
+}
+
+namespace {
+template <int MODE>
+cudaError_t launch_super_mode(const ReplaceParams& p, cudaStream_t st, int* grid_out) {
+  static std::mutex mu;
+  static unsigned long long attr_dev_mask = 0;
+  const uint32_t smem = make_layout_s(MODE, p.L, p.R, p.nsub).total;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!(attr_dev_mask & (1ull << (dev & 63)))) {
+      cudaError_t e = cudaFuncSetAttribute(replace_super_kernel<MODE>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      if (e != cudaSuccess) return e;
+      e = cudaFuncSetAttribute(query_super_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               200 * 1024);
+      if (e != cudaSuccess) return e;
+      attr_dev_mask |= 1ull << (dev & 63);
+    }
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, replace_super_kernel<MODE>, kThreads,
+                                                                smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  long long grid = (long long)per_sm * device_sm_count();
+  if (grid > (long long)p.num_tiles) grid = p.num_tiles;
+  if (grid < 1) grid = 1;
+  replace_super_kernel<MODE><<<(unsigned)grid, kThreads, smem, st>>>(p);
+  if (grid_out) *grid_out = (int)grid;
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_replace_super(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out) {
+  if (p.mode == kModeFree) return launch_super_mode<kModeFree>(p, st, grid_ctas_out);
+  return launch_super_mode<kModeSmall>(p, st, grid_ctas_out);
+}
+
+cudaError_t launch_query_super(const ReplaceParams& p, cudaStream_t st) {
+  const uint32_t smem = make_layout_s(kModeFree, p.L, p.R, 1).total;
+  if (p.mode == kModeFree)
+    query_super_kernel<kModeFree><<<1, kThreads, smem, st>>>(p);
+  else
+    query_super_kernel<kModeSmall><<<1, kThreads, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
 
 cudaError_t launch_replace(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out) {
   switch (p.mode) {

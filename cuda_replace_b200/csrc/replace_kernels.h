@@ -53,7 +53,8 @@ struct ApplyResult {              // device-side result block of one session
   unsigned int done_ctas;
   unsigned long long q_kept;      // query_prefix answer
   long long q_last;
-  unsigned long long pad[2];
+  unsigned long long last_tagged; // super-tile kernel: (epoch << 40) | (last kept start + 1), atomicMax
+  unsigned long long pad;
 };
 
 struct ReplaceParams {
@@ -72,11 +73,13 @@ struct ReplaceParams {
   unsigned int inv_l;             // ceil(65536 / L), for L < 64
   unsigned int query_limit;       // query kernel: tile-relative limit
   unsigned int query_tile;        // query kernel: tile index
-  unsigned int pad0;
+  unsigned int nsub;              // super-tile kernel: 16 KiB sub-tiles per super-tile (0 = tile kernel)
+  unsigned long long query_limit64;  // super-tile query: absolute limit
   unsigned int* status;           // [num_tiles]
   TileIncl* incl;                 // [num_tiles]
   unsigned long long* agg;        // [num_tiles * agg_entries]
   ApplyResult* res;
+  long long* tile_last;           // super-tile kernel: last kept start per super-tile or -1 [num_tiles]
   const uint8_t* pat_ext;         // device copy when L > kInlineMax
   const uint8_t* rep_ext;         // device copy when R > kInlineMax
   uint8_t pat[kInlineMax];
@@ -90,6 +93,12 @@ void prepare_pattern_fields(ReplaceParams& p, const uint8_t* pat, uint32_t L);
 uint32_t tile_kernel_smem_bytes(uint32_t mode, uint32_t L, uint32_t R);
 // Launch one apply. grid_ctas_out receives the number of CTAs launched.
 cudaError_t launch_replace(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out);
+// Sub-tiles per super-tile for the super-tile kernel, or 0 when (mode, L) needs the tile kernel.
+uint32_t super_nsub(uint32_t mode, uint32_t L);
+// Launch one apply with the super-tile kernel (p.nsub > 0, p.tile_last set).
+cudaError_t launch_replace_super(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out);
+// Query for an apply made by the super-tile kernel: p.query_limit64 = limit (< p.n).
+cudaError_t launch_query_super(const ReplaceParams& p, cudaStream_t st);
 // One CTA answers query_prefix for tile p.query_tile at tile-relative limit p.query_limit,
 // using the tile records of the apply described by p; writes res->q_kept / res->q_last.
 cudaError_t launch_query(const ReplaceParams& p, cudaStream_t st);
