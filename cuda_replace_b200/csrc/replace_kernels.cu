@@ -964,17 +964,19 @@ __device__ __forceinline__ uint32_t ld_u32_unaligned(const uint8_t* p) {
 }
 
 // Streams one thread's output bytes into the staging buffer: whole words are stored as
-// words; the partial first and last words (shared with the neighbouring threads) byte by byte.
+// words; the partial first and last words (shared with the neighbouring threads) byte by
+// byte. `pend` holds the nb (0..3) bytes of the current word not yet stored; appending four
+// bytes leaves nb unchanged, so the word loop has no branches.
 struct Emitter {
   uint32_t* stg;
-  unsigned long long acc;
-  uint32_t nb;    // bytes held in acc (the first `skip` of them belong to the previous thread)
-  uint32_t wpos;  // staging word of acc's first byte
-  uint32_t skip;
+  uint32_t pend;  // pending bytes (low nb bytes; the first `skip` belong to the previous thread)
+  uint32_t nb;
+  uint32_t wpos;  // staging word that pend will complete
+  uint32_t skip;  // nonzero until the first (partial) word has been stored
 
   __device__ __forceinline__ void init(uint32_t* s, uint32_t start_byte) {
     stg = s;
-    acc = 0;
+    pend = 0;
     nb = start_byte & 3u;
     wpos = start_byte >> 2;
     skip = nb;
@@ -990,42 +992,56 @@ struct Emitter {
     } else {
       stg[stg_pad(wpos)] = word;
     }
+    ++wpos;
   }
-  // append k (1..4) bytes held in the low bytes of v
-  __device__ __forceinline__ void append(uint32_t v, uint32_t k) {
-    acc |= (unsigned long long)(k == 4 ? v : (v & ((1u << (8 * k)) - 1u))) << (8 * nb);
-    nb += k;
-    if (nb >= 4) {
-      put_word((uint32_t)acc);
-      acc >>= 32;
-      nb -= 4;
-      ++wpos;
+  __device__ __forceinline__ void append4(uint32_t v) {
+    const uint32_t s = 8u * nb;
+    put_word(pend | (v << s));
+    pend = __funnelshift_rc(v, 0u, 32u - s);
+  }
+  __device__ __forceinline__ void append1(uint32_t b) {
+    pend |= (b & 0xFFu) << (8u * nb);
+    if (++nb == 4u) {
+      put_word(pend);
+      pend = 0;
+      nb = 0;
     }
   }
   __device__ __forceinline__ void finish() {
-    if (nb > skip) store_bytes((uint32_t)acc, skip, nb);
+    if (nb > skip) store_bytes(pend, skip, nb);
   }
 };
 
 // Literal bytes src[0, len) from shared memory.
 __device__ __forceinline__ void emit_literal(Emitter& e, const uint8_t* src, uint32_t len) {
   uint32_t i = 0;
-  for (; i + 4 <= len; i += 4) e.append(ld_u32_unaligned(src + i), 4);
-  for (; i < len; ++i) e.append(src[i], 1);
+  for (; i + 4 <= len; i += 4) e.append4(ld_u32_unaligned(src + i));
+  for (; i < len; ++i) e.append1(src[i]);
 }
 
 // r copies of the replacement: rrep holds the replacement repeated (at least R + 8 bytes);
-// step4 = 4 mod R.
+// step4 = 4 mod R. When R divides 4 every word of the run is the same.
 __device__ __forceinline__ void emit_repeat(Emitter& e, const uint8_t* rrep, uint32_t R, uint32_t step4,
                                             uint32_t r) {
-  uint32_t total = r * R, ph = 0;
-  for (; total >= 4; total -= 4) {
-    e.append(ld_u32_unaligned(rrep + ph), 4);
-    ph += step4;
-    if (ph >= R) ph -= R;
+  uint32_t total = r * R;
+  if (step4 == 0u) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(rrep);
+    for (; total >= 4; total -= 4) e.append4(w);
+  } else {
+    uint32_t ph = 0;
+    for (; total >= 4; total -= 4) {
+      e.append4(ld_u32_unaligned(rrep + ph));
+      ph += step4;
+      if (ph >= R) ph -= R;
+    }
+    for (; total; --total) {
+      e.append1(rrep[ph]);
+      if (++ph == R) ph = 0;
+    }
+    return;
   }
-  for (; total; --total) {
-    e.append(rrep[ph], 1);
+  for (uint32_t ph = 0; total; --total) {
+    e.append1(rrep[ph]);
     if (++ph == R) ph = 0;
   }
 }
@@ -1258,6 +1274,8 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   __shared__ uint32_t s_cin;
   __shared__ uint32_t s_fail;
   __shared__ uint32_t s_sub_lco[kMaxSub];
+  __shared__ uint32_t s_wcnt[kMaxSub * kWarps];   // kModeFree: kept count per (sub-tile, warp)
+  __shared__ uint32_t s_wcend[kMaxSub * kWarps];  // kModeFree: max cover end per (sub-tile, warp)
 
   const uint32_t L = p.L, R = p.R, nsub = p.nsub;
   const LayoutS lay = make_layout_s(MODE, L, R, nsub);
@@ -1329,17 +1347,19 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       if (L > 4) mask = verify_tail(mask, tb + sb, ps, L);
       masks[j * kThreads + tid] = mask;
       if (MODE == kModeFree) {
-        const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
-        const uint32_t cend = mask ? sb + last + L : 0u;
-        uint32_t tot_cend, tot_cnt;
-        (void)block_excl_scan(cend, 0u, OpMax(), s_scan, &tot_cend);
-        (void)block_excl_scan((uint32_t)__popcll(mask), 0u, OpSum(), s_scan, &tot_cnt);
-        if (tid == 0) {
-          const long long lco = tot_cend > (uint32_t)kTile ? (long long)(tot_cend - kTile) : 0ll;
-          s_sub_lco[j] = (uint32_t)lco;
-          const long long shifted = fr_lco - (long long)kTile;
-          fr_lco = shifted > lco ? shifted : lco;
-          fr_cnt += tot_cnt;
+        // every candidate is kept: the sub-tile needs only its count and how far its last
+        // match reaches past its end (warp reductions; folded by thread 0 after pass A)
+        uint32_t cnt = (uint32_t)__popcll(mask);
+        uint32_t cend = mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u;
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+          cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
+          const uint32_t o = __shfl_xor_sync(0xffffffffu, cend, d);
+          cend = o > cend ? o : cend;
+        }
+        if (lane == 0) {
+          s_wcnt[j * kWarps + warp] = cnt;
+          s_wcend[j * kWarps + warp] = cend;
         }
       } else {
         uint16_t* segtab = reinterpret_cast<uint16_t*>(smem + lay.segtab);
@@ -1387,6 +1407,19 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     // ================= publish the aggregate, look back, publish the inclusive prefix
     if (MODE == kModeFree) {
       if (tid == 0) {
+        for (uint32_t j = 0; j < m; ++j) {
+          uint32_t tot_cnt = 0, tot_cend = 0;
+          for (int w = 0; w < kWarps; ++w) {
+            tot_cnt += s_wcnt[j * kWarps + w];
+            const uint32_t ce = s_wcend[j * kWarps + w];
+            tot_cend = ce > tot_cend ? ce : tot_cend;
+          }
+          const long long lco = tot_cend > (uint32_t)kTile ? (long long)(tot_cend - kTile) : 0ll;
+          s_sub_lco[j] = (uint32_t)lco;
+          const long long shifted = fr_lco - (long long)kTile;
+          fr_lco = shifted > lco ? shifted : lco;
+          fr_cnt += tot_cnt;
+        }
         if (t > 0) {
           __stcg(p.agg + t, fr_cnt | ((unsigned long long)fr_lco << 32));
           __threadfence();
@@ -1455,12 +1488,25 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       uint64_t kept;
       uint32_t cnt;
       if (MODE == kModeFree) {
-        const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
-        const uint32_t cend = mask ? sb + last + L : 0u;
-        uint32_t tot;
-        const uint32_t pre = block_excl_scan(cend, 0u, OpMax(), s_scan, &tot);
-        const uint32_t cov = csub > pre ? csub : pre;
-        x_in = cov > sb ? cov - sb : 0u;
+        if (L <= 64u) {
+          // only the previous segment's last match (or the sub-tile carry) can reach here
+          uint32_t cov = tid == 0 ? csub : 0u;
+          if (tid > 0) {
+            const uint64_t pm = masks[j * kThreads + tid - 1];
+            if (pm) {
+              const uint32_t e = 63u - (uint32_t)__clzll((long long)pm) + L;
+              if (e > 64u && e - 64u > cov) cov = e - 64u;
+            }
+          }
+          x_in = cov;
+        } else {
+          const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
+          const uint32_t cend = mask ? sb + last + L : 0u;
+          uint32_t tot;
+          const uint32_t pre = block_excl_scan(cend, 0u, OpMax(), s_scan, &tot);
+          const uint32_t cov = csub > pre ? csub : pre;
+          x_in = cov > sb ? cov - sb : 0u;
+        }
         kept = mask;
         cnt = (uint32_t)__popcll(mask);
         const long long sh = (long long)csub - (long long)kTile;
