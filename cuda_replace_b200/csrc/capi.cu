@@ -123,6 +123,7 @@ struct Session {
   unsigned long long* agg = nullptr;
   size_t agg_cap = 0;
   long long* tile_last = nullptr;  // per super-tile (same capacity as status)
+  unsigned long long* rec = nullptr;  // 16-byte look-back record per super-tile
   ApplyResult* res = nullptr;       // device
   ApplyResult* res_host = nullptr;  // page-locked mirror
   uint8_t* ext = nullptr;           // device copy of long patterns / replacements
@@ -189,6 +190,16 @@ cudaError_t ensure_scratch(Session* s, size_t tiles, size_t entries_per_tile) {
       cudaFree(in);
       return e;
     }
+    unsigned long long* rc = nullptr;
+    e = cudaMalloc(&rc, cap * 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(rc, 0, cap * 2 * sizeof(unsigned long long), s->stream);
+    if (e != cudaSuccess) {
+      cudaFree(st);
+      cudaFree(in);
+      cudaFree(tl);
+      if (rc) cudaFree(rc);
+      return e;
+    }
     e = cudaMemsetAsync(st, 0, cap * sizeof(uint32_t), s->stream);
     if (e != cudaSuccess) {
       cudaFree(st);
@@ -198,9 +209,11 @@ cudaError_t ensure_scratch(Session* s, size_t tiles, size_t entries_per_tile) {
     if (s->status) cudaFree(s->status);
     if (s->incl) cudaFree(s->incl);
     if (s->tile_last) cudaFree(s->tile_last);
+    if (s->rec) cudaFree(s->rec);
     s->status = st;
     s->incl = in;
     s->tile_last = tl;
+    s->rec = rc;
     s->tiles_cap = cap;
   }
   const size_t entries = tiles * entries_per_tile;
@@ -217,10 +230,13 @@ cudaError_t ensure_scratch(Session* s, size_t tiles, size_t entries_per_tile) {
 }
 
 uint32_t next_epoch(Session* s) {
-  if (s->epoch >= (1u << 30) - 2) {
-    // wrap: clear every status word so old epochs cannot alias new ones
+  // Status words hold the epoch (30 bits), look-back records its low 24 bits: when either
+  // wraps, clear both so a stale word from 2^24 launches ago can never look current.
+  if (s->epoch >= (1u << 30) - 2 || ((s->epoch + 1) & 0xFFFFFFu) == 0) {
     cudaMemsetAsync(s->status, 0, s->tiles_cap * sizeof(uint32_t), s->stream);
-    s->epoch = 0;
+    if (s->rec) cudaMemsetAsync(s->rec, 0, s->tiles_cap * 2 * sizeof(unsigned long long), s->stream);
+    if (s->epoch >= (1u << 30) - 2) s->epoch = 0;
+    ++s->epoch;  // skip the value whose record tag would be 0
   }
   return ++s->epoch;
 }
@@ -234,6 +250,7 @@ void session_free(Session* s) {
   if (s->status) cudaFree(s->status);
   if (s->incl) cudaFree(s->incl);
   if (s->tile_last) cudaFree(s->tile_last);
+  if (s->rec) cudaFree(s->rec);
   if (s->agg) cudaFree(s->agg);
   if (s->res) cudaFree(s->res);
   if (s->res_host) cudaFreeHost(s->res_host);
@@ -385,6 +402,7 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
   e = ensure_scratch(s, tiles, p.agg_entries);
   if (e != cudaSuccess) return (int)e;
   p.tile_last = s->tile_last;
+  p.rec = s->rec;
 
   const size_t bound = output_bound(n, L, R);
   size_t want = bound;
@@ -692,6 +710,7 @@ CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size
   cudaError_t e = ensure_scratch(s, tiles, p.agg_entries);
   if (e != cudaSuccess) return (int)e;
   p.tile_last = s->tile_last;
+  p.rec = s->rec;
   memcpy(p.pat, pat, L);
   if (R) memcpy(p.rep, rep, R);
   p.in = d_in;

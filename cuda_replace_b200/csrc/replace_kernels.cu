@@ -1046,6 +1046,50 @@ __device__ __forceinline__ void emit_repeat(Emitter& e, const uint8_t* rrep, uin
   }
 }
 
+// ---- short bordered patterns (L <= 4): segment functions packed in registers.
+// Entry c (carry-in c) is 16 bits: kept count in bits 0-13, carry-out in bits 14-15; entries
+// 0,1 live in t0 and 2,3 in t1. Composition is a few selects, so a warp composes its 32
+// segment functions with a Kogge-Stone scan of shuffles instead of a 32-step walk.
+__device__ __forceinline__ uint32_t ks_get(uint32_t t0, uint32_t t1, uint32_t c) {
+  const uint32_t w = (c & 2u) ? t1 : t0;
+  return (c & 1u) ? (w >> 16) : (w & 0xFFFFu);
+}
+
+// (t0, t1) <- (t0, t1) after (o0, o1): the other function is applied first.
+__device__ __forceinline__ void ks_compose(uint32_t& t0, uint32_t& t1, uint32_t o0, uint32_t o1, uint32_t L) {
+  uint32_t r[4];
+#pragma unroll
+  for (uint32_t c = 0; c < 4; ++c) {
+    const uint32_t o = ks_get(o0, o1, c);
+    const uint32_t m = ks_get(t0, t1, o >> 14);
+    r[c] = c < L ? (((o & 0x3FFFu) + (m & 0x3FFFu)) | (m & 0xC000u)) : 0u;
+  }
+  t0 = r[0] | (r[1] << 16);
+  t1 = r[2] | (r[3] << 16);
+}
+
+// Block-wide exclusive scan with ONE barrier: buf alternates between two scratch arrays so
+// the next scan cannot overwrite totals still being read.
+template <typename Op>
+__device__ __forceinline__ uint32_t block_excl_scan1(uint32_t v, uint32_t identity, Op op, uint32_t* buf,
+                                                     uint32_t* total) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t inc = warp_incl_scan(v, op);
+  if (lane == 31) buf[warp] = inc;
+  __syncthreads();
+  uint32_t wpre = identity, tot = identity;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    const uint32_t s = buf[w];
+    if ((uint32_t)w < warp) wpre = op(wpre, s);
+    tot = op(tot, s);
+  }
+  uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) ex = identity;
+  *total = tot;
+  return op(wpre, ex);
+}
+
 // Warp-level bounded wait over the window of predecessors j = base - lane (j < 0 is the
 // virtual tile before tile 0, treated as inclusive with K = 0, carry = 0). Returns the lane
 // of the nearest inclusive tile (32 if none) once every nearer lane has at least its
@@ -1085,34 +1129,85 @@ __device__ __forceinline__ int warp_wait_window(const ReplaceParams& p, long lon
   }
 }
 
-// Mode free: a block's function is carry_out(c) = max(c - span, cover), count constant.
-// Look-back over super-tiles of S bytes by warp 0; returns (K, carry) for tile t.
-__device__ __forceinline__ bool lookback_free(const ReplaceParams& p, uint32_t t, unsigned long long S,
-                                              unsigned long long* K_out, uint32_t* c_out) {
+// ---- one-round-trip look-back records (kModeFree, and kModeSmall with L <= 4).
+// Tile t's record is 16 bytes, rec[2t] and rec[2t+1]; each word carries the launch tag
+// (low 24 bits of the epoch, bits 40-63) and the state (bits 38-39) next to 38 payload
+// bits, so a reader validates a record with one 16-byte load: both tags current and both
+// states equal (a torn read of an AGG -> INC update fails that test and is retried).
+// AGG payload: free mode (count, cover); small mode the 4-entry table (19 bits per entry:
+// count 17 bits, carry-out 2 bits). INC payload: (kept prefix, carry-out).
+__device__ __forceinline__ unsigned long long rec_word(uint32_t tag, uint32_t state, unsigned long long d) {
+  return ((unsigned long long)tag << 40) | ((unsigned long long)state << 38) | (d & ((1ull << 38) - 1ull));
+}
+__device__ __forceinline__ void rec_store(unsigned long long* rec, uint32_t t, unsigned long long w0,
+                                          unsigned long long w1) {
+  asm volatile("st.volatile.global.v2.u64 [%0], {%1, %2};" ::"l"(rec + 2ull * t), "l"(w0), "l"(w1) : "memory");
+}
+__device__ __forceinline__ void rec_load(const unsigned long long* rec, uint32_t t, unsigned long long* w0,
+                                         unsigned long long* w1) {
+  asm volatile("ld.volatile.global.v2.u64 {%0, %1}, [%2];" : "=l"(*w0), "=l"(*w1) : "l"(rec + 2ull * t) : "memory");
+}
+__device__ __forceinline__ unsigned long long rec_data(unsigned long long w) { return w & ((1ull << 38) - 1ull); }
+
+// Window of predecessors j = base - lane read from the records (j < 0: virtual inclusive
+// tile with zero payload). Returns the nearest inclusive lane (32 if none) once every
+// nearer lane holds a valid record, or -1 when the wait gave up; d0/d1 receive the payload.
+__device__ __forceinline__ int warp_read_window(const ReplaceParams& p, long long base, unsigned long long* d0,
+                                                unsigned long long* d1) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const long long j = base - (long long)lane;
+  const uint32_t tag = p.epoch & 0xFFFFFFu;
+  unsigned long long t0 = 0;
+  uint32_t ns = 32;
+  for (;;) {
+    uint32_t st = 0;
+    unsigned long long w0 = 0, w1 = 0;
+    if (j < 0) {
+      st = kStInc;
+    } else {
+      rec_load(p.rec, (uint32_t)j, &w0, &w1);
+      const uint32_t s0 = (uint32_t)(w0 >> 38) & 3u, s1 = (uint32_t)(w1 >> 38) & 3u;
+      if ((uint32_t)(w0 >> 40) == tag && (uint32_t)(w1 >> 40) == tag && s0 == s1) st = s0;
+    }
+    const uint32_t ready = __ballot_sync(0xffffffffu, st != 0);
+    const uint32_t incm = __ballot_sync(0xffffffffu, st == kStInc);
+    const uint32_t pl = incm ? (uint32_t)(__ffs(incm) - 1) : 32u;
+    const uint32_t need = pl == 32u ? 0xffffffffu : ((1u << pl) - 1u);
+    if ((ready & need) == need) {
+      *d0 = rec_data(w0);
+      *d1 = rec_data(w1);
+      return (int)pl;
+    }
+    if (aborted(p)) return -1;
+    const unsigned long long now = global_ns();
+    if (t0 == 0) {
+      t0 = now;
+    } else if (now - t0 > kSpinLimitNs) {
+      if (lane == 0) set_error(p);
+      return -1;
+    }
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+  }
+}
+
+__device__ __forceinline__ bool lookback_free_rec(const ReplaceParams& p, uint32_t t, unsigned long long S,
+                                                  unsigned long long* K_out, uint32_t* c_out) {
   const uint32_t lane = threadIdx.x & 31u;
   unsigned long long acc_cnt = 0;
   long long acc_cover = 0;
   unsigned long long acc_span = 0;
   long long base = (long long)t - 1;
   for (;;) {
-    const long long j = base - (long long)lane;
-    uint32_t st;
-    const int plr = warp_wait_window(p, base, &st);
+    unsigned long long d0, d1;
+    const int plr = warp_read_window(p, base, &d0, &d1);
     if (plr < 0) return false;
     const uint32_t pl = (uint32_t)plr;
     unsigned long long cnt = 0;
     long long val = LLONG_MIN / 4;
-    if (lane < pl) {
-      const unsigned long long e = __ldcg(p.agg + j);
-      cnt = e & 0xFFFFFFFFull;
-      val = (long long)(e >> 32) - (long long)(lane * S);
-    } else if (lane == pl) {
-      if (j >= 0) {
-        cnt = __ldcg(&p.incl[j].kept);
-        val = (long long)__ldcg(&p.incl[j].carry) - (long long)(lane * S);
-      } else {
-        val = 0;
-      }
+    if (lane <= pl && lane < 32u) {
+      cnt = d0;
+      val = (long long)d1 - (long long)(lane * S);
     }
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) {
@@ -1131,6 +1226,58 @@ __device__ __forceinline__ bool lookback_free(const ReplaceParams& p, uint32_t t
     acc_cover = cov > acc_cover ? cov : acc_cover;
     acc_cnt += cnt;
     acc_span += 32ull * S;
+    base -= 32;
+  }
+}
+
+// entry c of a packed 4-entry table (two 38-bit payloads)
+__device__ __forceinline__ uint32_t tab4_entry(unsigned long long d0, unsigned long long d1, uint32_t c) {
+  const unsigned long long w = (c & 2u) ? d1 : d0;
+  return (uint32_t)((c & 1u) ? (w >> 19) : w) & 0x7FFFFu;
+}
+
+__device__ __forceinline__ bool lookback_small4_rec(const ReplaceParams& p, uint32_t t, uint32_t L,
+                                                    unsigned long long* K_out, uint32_t* c_out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long acc_cnt = 0;  // lane c < L: function of the tiles between the window and t
+  uint32_t acc_carry = lane;
+  long long base = (long long)t - 1;
+  for (;;) {
+    unsigned long long d0, d1;
+    const int plr = warp_read_window(p, base, &d0, &d1);
+    if (plr < 0) return false;
+    const uint32_t pl = (uint32_t)plr;
+    if (pl < 32) {
+      unsigned long long K = __shfl_sync(0xffffffffu, d0, pl);
+      uint32_t x = (uint32_t)__shfl_sync(0xffffffffu, d1, pl);
+#pragma unroll
+      for (int i = 31; i >= 0; --i) {
+        if ((uint32_t)i < pl) {
+          const unsigned long long a = __shfl_sync(0xffffffffu, d0, i);
+          const unsigned long long b = __shfl_sync(0xffffffffu, d1, i);
+          const uint32_t e = tab4_entry(a, b, x);
+          K += e & 0x1FFFFu;
+          x = e >> 17;
+        }
+      }
+      *K_out = K + __shfl_sync(0xffffffffu, acc_cnt, x);
+      *c_out = __shfl_sync(0xffffffffu, acc_carry, x);
+      return true;
+    }
+    uint32_t y = lane < L ? lane : 0u;
+    unsigned long long wc = 0;
+#pragma unroll
+    for (int i = 31; i >= 0; --i) {
+      const unsigned long long a = __shfl_sync(0xffffffffu, d0, i);
+      const unsigned long long b = __shfl_sync(0xffffffffu, d1, i);
+      const uint32_t e = tab4_entry(a, b, y);
+      wc += e & 0x1FFFFu;
+      y = e >> 17;
+    }
+    const unsigned long long ac = __shfl_sync(0xffffffffu, acc_cnt, y);
+    const uint32_t ax = __shfl_sync(0xffffffffu, acc_carry, y);
+    acc_cnt = wc + ac;
+    acc_carry = ax;
     base -= 32;
   }
 }
@@ -1219,11 +1366,7 @@ struct LoadRing {
                                         unsigned long long n16, uint32_t want_a) {
     const uint32_t NT = p.num_tiles;
     while (issued - consumed < (uint32_t)kNBuf) {
-      if (iq >= 2) break;
-      if (iq == 1 && q[1] == 0xFFFFFFFFu) {
-        const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
-        q[1] = nx < NT ? nx : NT;
-      }
+      if (iq >= 1) break;  // loads of the next super-tile start once it is claimed
       const uint32_t tile = q[iq];
       if (tile >= NT) break;
       const uint32_t m = subs_in_tile(tile, S, p.n, p.nsub);
@@ -1261,14 +1404,14 @@ struct LoadRing {
     return smem + lay.in0 + b * lay.inbytes;
   }
   __device__ __forceinline__ void release() { ++consumed; }
-  __device__ __forceinline__ void shift() { iq = iq > 0 ? iq - 1 : 0; }
+  __device__ __forceinline__ void shift() { iq = 0; iph = 0; ij = 0; }
 };
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid_constant__ ReplaceParams p) {
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t s_bar[kNBuf];
-  __shared__ uint32_t s_scan[kWarps];
+  __shared__ uint32_t s_scan2[2][kWarps];  // alternating buffers of block_excl_scan1
   __shared__ uint32_t s_q[2];  // current and next super-tile of this CTA
   __shared__ unsigned long long s_kexcl;
   __shared__ uint32_t s_cin;
@@ -1299,6 +1442,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     for (uint32_t i = tid; i < R + 16; i += kThreads) rs[i] = R ? rsrc[i % R] : (uint8_t)0;
   }
   const uint32_t step4 = R ? 4u % R : 0u;
+  uint32_t nscan = 0;  // block_excl_scan1 calls so far (selects the scratch buffer)
 
   // ---- load ring: thread 0 issues loads in the order they will be consumed:
   // for each super-tile of this CTA, pass A (sub-tile + halo) then pass B (sub-tile).
@@ -1362,23 +1506,58 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           s_wcend[j * kWarps + warp] = cend;
         }
       } else {
-        uint16_t* segtab = reinterpret_cast<uint16_t*>(smem + lay.segtab);
-        build_seg_table16(mask, L, p.inv_l, p.stride_mask, segtab + tid * lay.rs);
-        __syncthreads();
         uint8_t* srec = smem + lay.srec + (size_t)j * kThreads * L;
         uint32_t* wtab = reinterpret_cast<uint32_t*>(smem + lay.wtab);
-        if (lane < L) {
-          uint32_t x = lane, cnt = 0;
-          const uint32_t seg0 = warp * 32u;
-#pragma unroll 8
-          for (uint32_t k = 0; k < 32; ++k) {
-            const uint32_t seg = seg0 + k;
-            srec[seg * L + lane] = (uint8_t)x;
-            const uint32_t v = segtab[seg * lay.rs + x];
-            cnt += v & 0xFFu;
-            x = v >> 8;
+        if (L <= 4u) {
+          // this segment's function in registers, then a Kogge-Stone scan over the warp
+          uint32_t ent[4];
+#pragma unroll
+          for (uint32_t c = 0; c < 4; ++c) {
+            ent[c] = 0;
+            if (c < L) {
+              const uint64_t mm = mask >> c;
+              if (mm) {
+                const uint32_t e = c + (uint32_t)(__ffsll((long long)mm) - 1);
+                const Walk w = seg_walk(mask, e, L, p.inv_l, p.stride_mask);
+                const uint32_t carry = w.end > 64 ? w.end - 64 : 0;
+                ent[c] = w.cnt | (carry << 14);
+              }
+            }
           }
-          wtab[warp * L + lane] = cnt | (x << 16);
+          uint32_t t0 = ent[0] | (ent[1] << 16), t1 = ent[2] | (ent[3] << 16);
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o0 = __shfl_up_sync(0xffffffffu, t0, d);
+            const uint32_t o1 = __shfl_up_sync(0xffffffffu, t1, d);
+            if (lane >= (uint32_t)d) ks_compose(t0, t1, o0, o1, L);
+          }
+          // carry into this segment for each warp carry-in: the exclusive prefix
+          uint32_t x0 = __shfl_up_sync(0xffffffffu, t0, 1), x1 = __shfl_up_sync(0xffffffffu, t1, 1);
+          for (uint32_t c = 0; c < L; ++c)
+            srec[tid * L + c] = (uint8_t)(lane == 0 ? c : (ks_get(x0, x1, c) >> 14));
+          if (lane == 31) {
+            for (uint32_t c = 0; c < L; ++c) {
+              const uint32_t v = ks_get(t0, t1, c);
+              wtab[warp * L + c] = (v & 0x3FFFu) | ((v >> 14) << 16);
+            }
+          }
+        } else {
+          uint16_t* segtab = reinterpret_cast<uint16_t*>(smem + lay.segtab);
+          build_seg_table16(mask, L, p.inv_l, p.stride_mask, segtab + tid * lay.rs);
+          __syncthreads();
+          if (lane < L) {
+            uint32_t x = lane, cnt = 0;
+            const uint32_t seg0 = warp * 32u;
+#pragma unroll 8
+            for (uint32_t k = 0; k < 32; ++k) {
+              const uint32_t seg = seg0 + k;
+              srec[seg * L + lane] = (uint8_t)x;
+              const uint32_t v = segtab[seg * lay.rs + x];
+              cnt += v & 0xFFu;
+              x = v >> 8;
+            }
+            wtab[warp * L + lane] = cnt | (x << 16);
+          }
         }
         __syncthreads();
         if (warp == 0) {
@@ -1405,6 +1584,8 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     }
 
     // ================= publish the aggregate, look back, publish the inclusive prefix
+    const bool use_rec = MODE == kModeFree || L <= 4u;
+    const uint32_t tag = p.epoch & 0xFFFFFFu;
     if (MODE == kModeFree) {
       if (tid == 0) {
         for (uint32_t j = 0; j < m; ++j) {
@@ -1420,11 +1601,17 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           fr_lco = shifted > lco ? shifted : lco;
           fr_cnt += tot_cnt;
         }
-        if (t > 0) {
-          __stcg(p.agg + t, fr_cnt | ((unsigned long long)fr_lco << 32));
-          __threadfence();
-          st_release_u32(p.status + t, (p.epoch << 2) | kStAgg);
-        }
+        if (t > 0)
+          rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
+      }
+    } else if (use_rec) {
+      if (warp == 0) {
+        // gather the 4-entry table (lane c holds entry c) into lane 0 and publish it
+        unsigned long long e = lane < L ? ((unsigned long long)sup_cnt | ((unsigned long long)sup_carry << 17)) : 0ull;
+        const unsigned long long e1 = __shfl_sync(0xffffffffu, e, 1), e2 = __shfl_sync(0xffffffffu, e, 2),
+                                 e3 = __shfl_sync(0xffffffffu, e, 3);
+        if (lane == 0 && t > 0)
+          rec_store(p.rec, t, rec_word(tag, kStAgg, e | (e1 << 19)), rec_word(tag, kStAgg, e2 | (e3 << 19)));
       }
     } else {
       if (warp == 0) {
@@ -1440,7 +1627,14 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       unsigned long long K = 0;
       uint32_t c = 0;
       bool ok = true;
-      if (t > 0) ok = MODE == kModeFree ? lookback_free(p, t, S, &K, &c) : lookback_small(p, t, L, &K, &c);
+      if (t > 0) {
+        if (MODE == kModeFree)
+          ok = lookback_free_rec(p, t, S, &K, &c);
+        else if (use_rec)
+          ok = lookback_small4_rec(p, t, L, &K, &c);
+        else
+          ok = lookback_small(p, t, L, &K, &c);
+      }
       if (!ok) {
         K = 0;
         c = 0;
@@ -1461,10 +1655,13 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         cout = __shfl_sync(0xffffffffu, sup_carry, c);
       }
       if (lane == 0) {
+        if (use_rec) rec_store(p.rec, t, rec_word(tag, kStInc, Kin), rec_word(tag, kStInc, cout));
         __stcg(&p.incl[t].kept, Kin);
         __stcg(&p.incl[t].carry, cout);
-        __threadfence();
-        st_release_u32(p.status + t, (p.epoch << 2) | kStInc);
+        if (!use_rec) {
+          __threadfence();
+          st_release_u32(p.status + t, (p.epoch << 2) | kStInc);
+        }
         s_kexcl = K;
         s_cin = c;
       }
@@ -1503,7 +1700,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
           const uint32_t cend = mask ? sb + last + L : 0u;
           uint32_t tot;
-          const uint32_t pre = block_excl_scan(cend, 0u, OpMax(), s_scan, &tot);
+          const uint32_t pre = block_excl_scan1(cend, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot);
           const uint32_t cov = csub > pre ? csub : pre;
           x_in = cov > sb ? cov - sb : 0u;
         }
@@ -1536,7 +1733,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       }
       const uint32_t olen = V - covered + cnt * R;
       uint32_t sub_olen;
-      const uint32_t ooff = block_excl_scan(olen, 0u, OpSum(), s_scan, &sub_olen);
+      const uint32_t ooff = block_excl_scan1(olen, 0u, OpSum(), s_scan2[nscan++ & 1u], &sub_olen);
       const bool fits = (O + sub_olen <= p.out_cap) && (O <= p.out_cap);
       if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
       uint32_t W[17];
@@ -1661,7 +1858,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     {
       const uint32_t last1 = last_abs >= 0 ? (uint32_t)((unsigned long long)last_abs - tstart + 1) : 0u;
       uint32_t tot_last1;
-      (void)block_excl_scan(last1, 0u, OpMax(), s_scan, &tot_last1);
+      (void)block_excl_scan1(last1, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot_last1);
       if (tid == 0) {
         const long long lastt = tot_last1 ? (long long)(tstart + tot_last1 - 1) : -1ll;
         __stcg(p.tile_last + t, lastt);
@@ -1675,12 +1872,11 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     }
     // advance the queue
     if (tid == 0) {
-      s_q[0] = s_q[1] == 0xFFFFFFFFu ? 0xFFFFFFFFu : s_q[1];
+      // claim the next super-tile only now, when its pass A starts: a super-tile claimed
+      // early but started late would hold up the look-back of every later super-tile
+      const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
+      s_q[0] = nx < NT ? nx : NT;
       s_q[1] = 0xFFFFFFFFu;
-      if (s_q[0] == 0xFFFFFFFFu) {
-        const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
-        s_q[0] = nx < NT ? nx : NT;
-      }
       ring.shift();
       s_fail = 0;
       ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);

@@ -80,6 +80,7 @@ struct ReplaceParams {
   unsigned long long* agg;        // [num_tiles * agg_entries]
   ApplyResult* res;
   long long* tile_last;           // super-tile kernel: last kept start per super-tile or -1 [num_tiles]
+  unsigned long long* rec;        // super-tile kernel: 16-byte look-back record per super-tile [2 * num_tiles]
   const uint8_t* pat_ext;         // device copy when L > kInlineMax
   const uint8_t* rep_ext;         // device copy when R > kInlineMax
   uint8_t pat[kInlineMax];
