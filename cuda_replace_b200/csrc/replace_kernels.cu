@@ -852,9 +852,9 @@ constexpr int kNBuf = 2;
 constexpr int kMaxSub = 8;
 
 struct LayoutS {
-  uint32_t in0, outb, masks, pat, rep, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
+  uint32_t in0, outb, masks, pat, rep, tab16, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
   uint32_t rs, inbytes;
-  uint32_t stage_bytes;  // output bytes the padded staging buffer holds
+  uint32_t wstage_words;  // padded staging words per warp (its 2 KiB of input may grow 3x)
 };
 
 // Output bytes one 16 KiB sub-tile can produce, capped at three times its input.
@@ -870,23 +870,30 @@ __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_
   s.inbytes = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16) + 32;
   s.in0 = off;
   off += kNBuf * s.inbytes;
-  s.stage_bytes = kTile * stage_ratio(L, R) + 64;
+  {
+    const uint32_t words = (2048u * stage_ratio(L, R) + 48u) / 4u;
+    s.wstage_words = words + words / 32u + 2u;
+  }
   s.outb = off;
-  off += align_up_u32((s.stage_bytes / 4 + s.stage_bytes / 128 + 2) * 4, 16);
+  off += align_up_u32(kWarps * s.wstage_words * 4u, 16);
   s.masks = off;
   off += nsub * kThreads * 8;
   s.pat = off;
   off += align_up_u32(L ? L : 1, 16);
   s.rep = off;
   off += align_up_u32(R + 16, 16);
+  s.tab16 = off;  // replacement repeated, 16 bytes from every phase (R <= 64)
+  off += (R >= 1 && R <= 64) ? R * 16 : 0;
   if (mode == kModeSmall) {
     s.rs = L | 1u;
-    s.segtab = off;
-    off += align_up_u32(kThreads * s.rs * 2, 16);
+    if (L > 4) {
+      s.segtab = off;
+      off += align_up_u32(kThreads * s.rs * 2, 16);
+    }
     s.srec = off;
     off += align_up_u32(nsub * kThreads * L, 16);
     s.wtab = off;
-    off += align_up_u32(kWarps * L * 4, 16);
+    off += align_up_u32(nsub * kWarps * L * 4, 16);
     s.wrec = off;
     off += align_up_u32(nsub * kWarps * L, 16);
     s.subrec = off;
@@ -1053,19 +1060,6 @@ __device__ __forceinline__ void emit_repeat(Emitter& e, const uint8_t* rrep, uin
 __device__ __forceinline__ uint32_t ks_get(uint32_t t0, uint32_t t1, uint32_t c) {
   const uint32_t w = (c & 2u) ? t1 : t0;
   return (c & 1u) ? (w >> 16) : (w & 0xFFFFu);
-}
-
-// (t0, t1) <- (t0, t1) after (o0, o1): the other function is applied first.
-__device__ __forceinline__ void ks_compose(uint32_t& t0, uint32_t& t1, uint32_t o0, uint32_t o1, uint32_t L) {
-  uint32_t r[4];
-#pragma unroll
-  for (uint32_t c = 0; c < 4; ++c) {
-    const uint32_t o = ks_get(o0, o1, c);
-    const uint32_t m = ks_get(t0, t1, o >> 14);
-    r[c] = c < L ? (((o & 0x3FFFu) + (m & 0x3FFFu)) | (m & 0xC000u)) : 0u;
-  }
-  t0 = r[0] | (r[1] << 16);
-  t1 = r[2] | (r[3] << 16);
 }
 
 // Block-wide exclusive scan with ONE barrier: buf alternates between two scratch arrays so
@@ -1341,6 +1335,105 @@ __device__ __forceinline__ bool lookback_small(const ReplaceParams& p, uint32_t 
   }
 }
 
+template <int LL>
+__device__ __forceinline__ void ks_compose_n(uint32_t& t0, uint32_t& t1, uint32_t o0, uint32_t o1) {
+  uint32_t r[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
+    const uint32_t o = ks_get(o0, o1, c);
+    const uint32_t m = ks_get(t0, t1, o >> 14);
+    r[c] = ((o & 0x3FFFu) + (m & 0x3FFFu)) | (m & 0xC000u);
+  }
+  t0 = r[0] | (r[1] << 16);
+  t1 = r[2] | (r[3] << 16);
+}
+
+// Kogge-Stone scan of the warp's 32 segment functions (L = LL <= 4): srec row of this
+// segment (carry into it for each warp carry-in) and, from lane 31, the warp function.
+template <int LL>
+__device__ __forceinline__ void ks_warp_tables(uint64_t mask, uint32_t inv_l, uint64_t stride, uint8_t* srec_row,
+                                               uint32_t* wtab_row) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t ent[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
+    const uint64_t mm = mask >> c;
+    if (mm) {
+      const uint32_t e = c + (uint32_t)(__ffsll((long long)mm) - 1);
+      const Walk w = seg_walk(mask, e, LL, inv_l, stride);
+      const uint32_t carry = w.end > 64 ? w.end - 64 : 0;
+      ent[c] = w.cnt | (carry << 14);
+    }
+  }
+  uint32_t t0 = ent[0] | (ent[1] << 16), t1 = ent[2] | (ent[3] << 16);
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o0 = __shfl_up_sync(0xffffffffu, t0, d);
+    const uint32_t o1 = __shfl_up_sync(0xffffffffu, t1, d);
+    if (lane >= (uint32_t)d) ks_compose_n<LL>(t0, t1, o0, o1);
+  }
+  const uint32_t x0 = __shfl_up_sync(0xffffffffu, t0, 1), x1 = __shfl_up_sync(0xffffffffu, t1, 1);
+#pragma unroll
+  for (uint32_t c = 0; c < (uint32_t)LL; ++c)
+    srec_row[c] = (uint8_t)(lane == 0 ? c : (ks_get(x0, x1, c) >> 14));
+  if (lane == 31) {
+#pragma unroll
+    for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
+      const uint32_t v = ks_get(t0, t1, c);
+      wtab_row[c] = (v & 0x3FFFu) | ((v >> 14) << 16);
+    }
+  }
+}
+
+// 16 bytes starting r = 4q + sh/8 bytes into the 32 bytes (A, B); q is warp-uniform.
+__device__ __forceinline__ uint4 extract16(const uint4& A, const uint4& B, uint32_t q, uint32_t sh) {
+  uint4 o;
+  switch (q) {
+    case 0:
+      o.x = __funnelshift_r(A.x, A.y, sh); o.y = __funnelshift_r(A.y, A.z, sh);
+      o.z = __funnelshift_r(A.z, A.w, sh); o.w = __funnelshift_r(A.w, B.x, sh);
+      break;
+    case 1:
+      o.x = __funnelshift_r(A.y, A.z, sh); o.y = __funnelshift_r(A.z, A.w, sh);
+      o.z = __funnelshift_r(A.w, B.x, sh); o.w = __funnelshift_r(B.x, B.y, sh);
+      break;
+    case 2:
+      o.x = __funnelshift_r(A.z, A.w, sh); o.y = __funnelshift_r(A.w, B.x, sh);
+      o.z = __funnelshift_r(B.x, B.y, sh); o.w = __funnelshift_r(B.y, B.z, sh);
+      break;
+    default:
+      o.x = __funnelshift_r(A.w, B.x, sh); o.y = __funnelshift_r(B.x, B.y, sh);
+      o.z = __funnelshift_r(B.y, B.z, sh); o.w = __funnelshift_r(B.z, B.w, sh);
+      break;
+  }
+  return o;
+}
+
+// Exclusive / inclusive scan over lanes 0..7 (the warps of a CTA), done by every warp.
+__device__ __forceinline__ void lanes8_sum(uint32_t v, uint32_t* excl, uint32_t* incl) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t x = lane < 8u ? v : 0u;
+#pragma unroll
+  for (int d = 1; d < 8; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= (uint32_t)d) x += o;
+  }
+  *incl = x;
+  uint32_t e = __shfl_up_sync(0xffffffffu, x, 1);
+  *excl = lane == 0 ? 0u : e;
+}
+__device__ __forceinline__ uint32_t lanes8_excl_max(uint32_t v) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t x = lane < 8u ? v : 0u;
+#pragma unroll
+  for (int d = 1; d < 8; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= (uint32_t)d) x = o > x ? o : x;
+  }
+  const uint32_t e = __shfl_up_sync(0xffffffffu, x, 1);
+  return lane == 0 ? 0u : e;
+}
+
 }  // namespace
 
 // Number of 16 KiB sub-tiles in super-tile `tile`.
@@ -1412,7 +1505,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t s_bar[kNBuf];
   __shared__ uint32_t s_scan2[2][kWarps];  // alternating buffers of block_excl_scan1
-  __shared__ uint32_t s_q[2];  // current and next super-tile of this CTA
+  __shared__ uint32_t s_q[2];               // the super-tile this CTA works on
   __shared__ unsigned long long s_kexcl;
   __shared__ uint32_t s_cin;
   __shared__ uint32_t s_fail;
@@ -1433,6 +1526,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   const unsigned long long S = (unsigned long long)nsub * kTile;
   const uint32_t want_a = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16);
   const uint32_t NT = p.num_tiles;
+  const bool warp_stage = R <= 3u * L;  // every warp's output fits its staging area
 
   {
     const uint8_t* psrc = L <= (uint32_t)kInlineMax ? p.pat : p.pat_ext;
@@ -1441,11 +1535,18 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     // the replacement repeated: rs[i] = rep[i mod R] for i < R + 16
     for (uint32_t i = tid; i < R + 16; i += kThreads) rs[i] = R ? rsrc[i % R] : (uint8_t)0;
   }
+  const bool rep_table = R >= 1u && R <= 64u;
+  if (rep_table) {
+    const uint8_t* rsrc = R <= (uint32_t)kInlineMax ? p.rep : p.rep_ext;
+    uint8_t* t16 = smem + lay.tab16;
+    for (uint32_t i = tid; i < R * 16u; i += kThreads) t16[i] = rsrc[((i >> 4) + (i & 15u)) % R];
+  }
   const uint32_t step4 = R ? 4u % R : 0u;
+  const uint32_t step512 = R ? 512u % R : 0u;
   uint32_t nscan = 0;  // block_excl_scan1 calls so far (selects the scratch buffer)
 
-  // ---- load ring: thread 0 issues loads in the order they will be consumed:
-  // for each super-tile of this CTA, pass A (sub-tile + halo) then pass B (sub-tile).
+  // ---- load ring: thread 0 issues loads in the order they are consumed: for the current
+  // super-tile, pass A (sub-tile + halo) then pass B (sub-tile).
   LoadRing ring;
   ring.init();
   if (tid == 0) {
@@ -1466,10 +1567,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     const uint32_t m = subs_in_tile(t, S, n, nsub);
     const unsigned long long tstart = (unsigned long long)t * S;
 
-    // ================= pass A: candidates and the super-tile function
-    uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 0, lane = carry
-    unsigned long long fr_cnt = 0;           // kModeFree: thread 0
-    long long fr_lco = 0;
+    // ================= pass A: candidates and per-warp functions of every sub-tile
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
@@ -1491,8 +1589,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       if (L > 4) mask = verify_tail(mask, tb + sb, ps, L);
       masks[j * kThreads + tid] = mask;
       if (MODE == kModeFree) {
-        // every candidate is kept: the sub-tile needs only its count and how far its last
-        // match reaches past its end (warp reductions; folded by thread 0 after pass A)
+        // every candidate is kept: per warp, the count and how far its last match reaches
         uint32_t cnt = (uint32_t)__popcll(mask);
         uint32_t cend = mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u;
 #pragma unroll
@@ -1507,44 +1604,19 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         }
       } else {
         uint8_t* srec = smem + lay.srec + (size_t)j * kThreads * L;
-        uint32_t* wtab = reinterpret_cast<uint32_t*>(smem + lay.wtab);
-        if (L <= 4u) {
-          // this segment's function in registers, then a Kogge-Stone scan over the warp
-          uint32_t ent[4];
-#pragma unroll
-          for (uint32_t c = 0; c < 4; ++c) {
-            ent[c] = 0;
-            if (c < L) {
-              const uint64_t mm = mask >> c;
-              if (mm) {
-                const uint32_t e = c + (uint32_t)(__ffsll((long long)mm) - 1);
-                const Walk w = seg_walk(mask, e, L, p.inv_l, p.stride_mask);
-                const uint32_t carry = w.end > 64 ? w.end - 64 : 0;
-                ent[c] = w.cnt | (carry << 14);
-              }
-            }
-          }
-          uint32_t t0 = ent[0] | (ent[1] << 16), t1 = ent[2] | (ent[3] << 16);
-#pragma unroll
-          for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t o0 = __shfl_up_sync(0xffffffffu, t0, d);
-            const uint32_t o1 = __shfl_up_sync(0xffffffffu, t1, d);
-            if (lane >= (uint32_t)d) ks_compose(t0, t1, o0, o1, L);
-          }
-          // carry into this segment for each warp carry-in: the exclusive prefix
-          uint32_t x0 = __shfl_up_sync(0xffffffffu, t0, 1), x1 = __shfl_up_sync(0xffffffffu, t1, 1);
-          for (uint32_t c = 0; c < L; ++c)
-            srec[tid * L + c] = (uint8_t)(lane == 0 ? c : (ks_get(x0, x1, c) >> 14));
-          if (lane == 31) {
-            for (uint32_t c = 0; c < L; ++c) {
-              const uint32_t v = ks_get(t0, t1, c);
-              wtab[warp * L + c] = (v & 0x3FFFu) | ((v >> 14) << 16);
-            }
-          }
+        uint32_t* wtab = reinterpret_cast<uint32_t*>(smem + lay.wtab) + (size_t)(j * kWarps + warp) * L;
+        if (L == 2u) {
+          ks_warp_tables<2>(mask, p.inv_l, p.stride_mask, srec + tid * 2u, wtab);
+        } else if (L == 3u) {
+          ks_warp_tables<3>(mask, p.inv_l, p.stride_mask, srec + tid * 3u, wtab);
+        } else if (L == 4u) {
+          ks_warp_tables<4>(mask, p.inv_l, p.stride_mask, srec + tid * 4u, wtab);
         } else {
+          // segment tables in shared memory, then lanes-over-carries walks of the warp's
+          // own 32 segments (only rows of this warp are read: a warp barrier suffices)
           uint16_t* segtab = reinterpret_cast<uint16_t*>(smem + lay.segtab);
           build_seg_table16(mask, L, p.inv_l, p.stride_mask, segtab + tid * lay.rs);
-          __syncthreads();
+          __syncwarp();
           if (lane < L) {
             uint32_t x = lane, cnt = 0;
             const uint32_t seg0 = warp * 32u;
@@ -1556,26 +1628,8 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
               cnt += v & 0xFFu;
               x = v >> 8;
             }
-            wtab[warp * L + lane] = cnt | (x << 16);
+            wtab[lane] = cnt | (x << 16);
           }
-        }
-        __syncthreads();
-        if (warp == 0) {
-          uint8_t* wrec = smem + lay.wrec + (size_t)j * kWarps * L;
-          uint32_t y = lane < L ? lane : 0u, cnt = 0;
-#pragma unroll
-          for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
-            if (lane < L) wrec[w * L + lane] = (uint8_t)y;
-            const uint32_t v = wtab[w * L + y];
-            cnt += v & 0xFFFFu;
-            y = v >> 16;
-          }
-          // compose the sub-tile function into the super-tile function
-          if (lane < L) (smem + lay.subrec)[j * L + lane] = (uint8_t)sup_carry;
-          const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
-          const uint32_t tx = __shfl_sync(0xffffffffu, y, sup_carry);
-          sup_cnt += tc;
-          sup_carry = tx;
         }
       }
       __syncthreads();
@@ -1583,9 +1637,12 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
     }
 
-    // ================= publish the aggregate, look back, publish the inclusive prefix
+    // ================= fold the sub-tiles into the super-tile function
     const bool use_rec = MODE == kModeFree || L <= 4u;
     const uint32_t tag = p.epoch & 0xFFFFFFu;
+    unsigned long long fr_cnt = 0;  // kModeFree: thread 0
+    long long fr_lco = 0;
+    uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 0, lane = carry-in
     if (MODE == kModeFree) {
       if (tid == 0) {
         for (uint32_t j = 0; j < m; ++j) {
@@ -1604,17 +1661,31 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         if (t > 0)
           rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
       }
-    } else if (use_rec) {
-      if (warp == 0) {
-        // gather the 4-entry table (lane c holds entry c) into lane 0 and publish it
+    } else if (warp == 0) {
+      const uint32_t* wt = reinterpret_cast<const uint32_t*>(smem + lay.wtab);
+      for (uint32_t j = 0; j < m; ++j) {
+        uint8_t* wrec = smem + lay.wrec + (size_t)j * kWarps * L;
+        uint32_t y = lane < L ? lane : 0u, cnt = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
+          if (lane < L) wrec[w * L + lane] = (uint8_t)y;
+          const uint32_t v = wt[(j * kWarps + w) * L + y];
+          cnt += v & 0xFFFFu;
+          y = v >> 16;
+        }
+        if (lane < L) (smem + lay.subrec)[j * L + lane] = (uint8_t)sup_carry;
+        const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
+        const uint32_t tx = __shfl_sync(0xffffffffu, y, sup_carry);
+        sup_cnt += tc;
+        sup_carry = tx;
+      }
+      if (use_rec) {
         unsigned long long e = lane < L ? ((unsigned long long)sup_cnt | ((unsigned long long)sup_carry << 17)) : 0ull;
         const unsigned long long e1 = __shfl_sync(0xffffffffu, e, 1), e2 = __shfl_sync(0xffffffffu, e, 2),
                                  e3 = __shfl_sync(0xffffffffu, e, 3);
         if (lane == 0 && t > 0)
           rec_store(p.rec, t, rec_word(tag, kStAgg, e | (e1 << 19)), rec_word(tag, kStAgg, e2 | (e3 << 19)));
-      }
-    } else {
-      if (warp == 0) {
+      } else {
         if (t > 0 && lane < L)
           __stcg(p.agg + (unsigned long long)t * L + lane, (unsigned long long)sup_cnt |
                                                                 ((unsigned long long)sup_carry << 32));
@@ -1623,6 +1694,8 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         if (t > 0 && lane == 0) st_release_u32(p.status + t, (p.epoch << 2) | kStAgg);
       }
     }
+
+    // ================= look back, publish the inclusive prefix
     if (warp == 0) {
       unsigned long long K = 0;
       uint32_t c = 0;
@@ -1640,7 +1713,6 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         c = 0;
         if (lane == 0) s_fail = 1;
       }
-      // own inclusive prefix
       unsigned long long Kin;
       uint32_t cout;
       if (MODE == kModeFree) {
@@ -1673,18 +1745,28 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     unsigned long long O = (unsigned long long)((long long)(tstart + cin) + (long long)kexcl * delta);
     const bool failed = s_fail != 0;
 
-    // ================= pass B: exact kept starts and output
-    uint32_t csub = cin;        // kModeFree: carry into sub-tile j
-    long long last_abs = -1;    // last kept start seen by this thread
+    // ================= pass B: exact kept starts and output, one warp region at a time
+    uint32_t csub = cin;      // kModeFree: carry into sub-tile j
+    long long last_abs = -1;  // last kept start seen by this thread
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
       const unsigned long long gseg = sstart + sb;
       const uint64_t mask = masks[j * kThreads + tid];
-      uint32_t x_in;
+      // valid input bytes of warp region `lane` (lanes 0..7 stand for the 8 warps)
+      const unsigned long long wrs = sstart + (unsigned long long)lane * 2048u;
+      const uint32_t wbytes = wrs >= n ? 0u : ((n - wrs) < 2048ull ? (uint32_t)(n - wrs) : 2048u);
+      uint32_t x_in, cnt, wolen = 0;
       uint64_t kept;
-      uint32_t cnt;
       if (MODE == kModeFree) {
+        const uint32_t wc = lane < 8u ? s_wcnt[j * kWarps + lane] : 0u;
+        const uint32_t we = lane < 8u ? s_wcend[j * kWarps + lane] : 0u;
+        const uint32_t pre = lanes8_excl_max(we);  // max cover end of the earlier warps
+        const uint32_t covs = csub > pre ? csub : pre;
+        const uint32_t wlo = lane * 2048u, whi = wlo + 2048u;
+        const uint32_t wcov = covs > wlo ? covs - wlo : 0u;
+        const uint32_t over = we > whi ? we - whi : 0u;
+        wolen = wbytes - (wcov < wbytes ? wcov : wbytes) - wc * L + over + wc * R;
         if (L <= 64u) {
           // only the previous segment's last match (or the sub-tile carry) can reach here
           uint32_t cov = tid == 0 ? csub : 0u;
@@ -1697,12 +1779,17 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           }
           x_in = cov;
         } else {
-          const uint32_t last = mask ? 63u - (uint32_t)__clzll((long long)mask) : 0u;
-          const uint32_t cend = mask ? sb + last + L : 0u;
-          uint32_t tot;
-          const uint32_t pre = block_excl_scan1(cend, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot);
-          const uint32_t cov = csub > pre ? csub : pre;
-          x_in = cov > sb ? cov - sb : 0u;
+          uint32_t ce = mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, ce, d);
+            if (lane >= (uint32_t)d) ce = o > ce ? o : ce;
+          }
+          uint32_t prev = __shfl_up_sync(0xffffffffu, ce, 1);
+          if (lane == 0) prev = 0;
+          const uint32_t pw = __shfl_sync(0xffffffffu, covs, warp);
+          const uint32_t cv = prev > pw ? prev : pw;
+          x_in = cv > sb ? cv - sb : 0u;
         }
         kept = mask;
         cnt = (uint32_t)__popcll(mask);
@@ -1712,8 +1799,17 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         csub = nx > 0 ? (uint32_t)nx : 0u;
       } else {
         const uint32_t cs = (smem + lay.subrec)[j * L + cin];
-        const uint32_t cw = (smem + lay.wrec)[((size_t)j * kWarps + warp) * L + cs];
-        x_in = (smem + lay.srec)[((size_t)j * kThreads + tid) * L + cw];
+        const uint8_t* wrec = smem + lay.wrec + (size_t)j * kWarps * L;
+        const uint32_t* wt = reinterpret_cast<const uint32_t*>(smem + lay.wtab) + (size_t)j * kWarps * L;
+        uint32_t cw = 0;
+        if (lane < 8u) {
+          cw = wrec[lane * L + cs];
+          const uint32_t e = wt[lane * L + cw];
+          const uint32_t wc = e & 0xFFFFu, co = e >> 16;
+          wolen = wbytes - (cw < wbytes ? cw : wbytes) - wc * L + co + wc * R;
+        }
+        const uint32_t mycw = __shfl_sync(0xffffffffu, cw, warp);
+        x_in = (smem + lay.srec)[((size_t)j * kThreads + tid) * L + mycw];
         if (x_in >= 64u) {
           kept = 0;
           cnt = 0;
@@ -1723,6 +1819,11 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           cnt = w.cnt;
         }
       }
+      uint32_t wbase, sub_total;
+      lanes8_sum(wolen, &wbase, &sub_total);
+      wbase = __shfl_sync(0xffffffffu, wbase, warp);
+      sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
+
       const uint32_t V = gseg >= n ? 0u : ((n - gseg) < 64ull ? (uint32_t)(n - gseg) : 64u);
       uint32_t covered = x_in < V ? x_in : V;
       if (cnt) {
@@ -1732,18 +1833,74 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         last_abs = (long long)(gseg + lastk);
       }
       const uint32_t olen = V - covered + cnt * R;
-      uint32_t sub_olen;
-      const uint32_t ooff = block_excl_scan1(olen, 0u, OpSum(), s_scan2[nscan++ & 1u], &sub_olen);
-      const bool fits = (O + sub_olen <= p.out_cap) && (O <= p.out_cap);
+      uint32_t toff = warp_incl_scan(olen, OpSum());
+      const uint32_t wtot = __shfl_sync(0xffffffffu, toff, 31);
+      toff -= olen;  // exclusive offset inside the warp region
+
+      const bool fits = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
       if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
-      uint32_t W[17];
-      load_seg_words(tb + sb, W);
-      const uint32_t sh = (uint32_t)(O & 15ull);
-      if (fits && !failed && sh + sub_olen + 16u <= lay.stage_bytes) {
-        // ---- assemble this sub-tile's output in the padded staging buffer
-        uint32_t* stg = reinterpret_cast<uint32_t*>(ob);
-        uint8_t* sbytes = ob;
-        const uint32_t cur = sh + ooff;
+      // warp output mode: no kept match in the warp (a copy of its input), or no literal byte
+      // (a run of replacements), or mixed
+      const uint32_t notlit = __ballot_sync(0xffffffffu, cnt != 0u || (lane > 0u && x_in != 0u));
+      const uint32_t notrep = __ballot_sync(0xffffffffu, olen != cnt * R);
+      if (fits && !failed && warp_stage && wtot != 0u && (notlit == 0u || (notrep == 0u && rep_table))) {
+        const unsigned long long g0 = O + wbase;
+        const unsigned long long ga = g0 & ~15ull;
+        const unsigned long long gend = g0 + wtot;
+        const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);  // first whole 16-byte chunk
+        const uint32_t c1 = (uint32_t)((gend - ga) >> 4);        // end of the whole chunks
+        if (notlit == 0u) {
+          // ---- LITERAL: output = input bytes [warp start + x0, ...): aligned 16-byte copies
+          const uint32_t x0 = __shfl_sync(0xffffffffu, x_in, 0);
+          const uint32_t srcw = warp * 2048u + x0;  // tile byte of the region's first output byte
+          const uint32_t off0 = srcw + (uint32_t)(ga + ((unsigned long long)c0 << 4) - g0);
+          const uint32_t r = off0 & 15u, q = r >> 2, sh = (r & 3u) * 8u;
+          for (uint32_t c = c0 + lane; c < c1; c += 32u) {
+            const uint32_t a = off0 - r + ((c - c0) << 4);
+            const uint4 A = *reinterpret_cast<const uint4*>(tb + a);
+            const uint4 B = *reinterpret_cast<const uint4*>(tb + a + 16u);
+            *reinterpret_cast<uint4*>(p.out + ga + ((unsigned long long)c << 4)) = extract16(A, B, q, sh);
+          }
+          unsigned long long b;
+          bool ok;
+          if (c0 < c1) {
+            b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
+            ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
+          } else {
+            b = g0 + lane;
+            ok = b < gend;
+          }
+          if (ok) p.out[b] = tb[srcw + (uint32_t)(b - g0)];
+        } else {
+          // ---- REPLACE: output = the replacement repeated, 16 bytes per phase from a table
+          const uint4* t16 = reinterpret_cast<const uint4*>(smem + lay.tab16);
+          uint32_t c = c0 + lane;
+          uint32_t ph = (uint32_t)((ga + ((unsigned long long)c << 4) - g0) % R);
+          for (; c < c1; c += 32u) {
+            *reinterpret_cast<uint4*>(p.out + ga + ((unsigned long long)c << 4)) = t16[ph];
+            ph += step512;
+            if (ph >= R) ph -= R;
+          }
+          unsigned long long b;
+          bool ok;
+          if (c0 < c1) {
+            b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
+            ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
+          } else {
+            b = g0 + lane;
+            ok = b < gend;
+          }
+          if (ok) p.out[b] = rs[(uint32_t)((b - g0) % R)];
+        }
+      } else if (fits && !failed && warp_stage) {
+        uint32_t W[17];
+        load_seg_words(tb + sb, W);
+        // ---- this warp's output: assemble in its padded staging area, then copy out
+        uint32_t* stg = reinterpret_cast<uint32_t*>(ob) + (size_t)warp * lay.wstage_words;
+        uint8_t* sbytes = reinterpret_cast<uint8_t*>(stg);
+        const unsigned long long g0 = O + wbase;
+        const unsigned long long ga = g0 & ~15ull;
+        const uint32_t cur = (uint32_t)(g0 - ga) + toff;
         if (olen && kept == 0 && x_in == 0 && V == 64u) {
           // literal-only segment: its 64 input bytes, shifted to the output word grid
           const uint32_t d = (4u - (cur & 3u)) & 3u;
@@ -1785,28 +1942,42 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           }
           e.finish();
         }
-        __syncthreads();
-        // ---- copy out: coalesced 16-byte stores; partial chunks at both ends byte by byte
-        const unsigned long long base_g = O - sh;
-        const uint32_t total = sh + sub_olen;
-        const uint32_t nch = (total + 15u) >> 4;
-        for (uint32_t c = tid; c < nch; c += kThreads) {
-          const uint32_t lo = c << 4, hi = lo + 16u;
-          if (lo >= sh && hi <= total) {
-            const uint32_t w = c << 2;
-            uint4 v;
-            v.x = stg[stg_pad(w)];
-            v.y = stg[stg_pad(w + 1)];
-            v.z = stg[stg_pad(w + 2)];
-            v.w = stg[stg_pad(w + 3)];
-            *reinterpret_cast<uint4*>(p.out + base_g + lo) = v;
+        __syncwarp();
+        // coalesced 16-byte stores for the whole chunks; the partial chunks at both ends of
+        // the region one byte per lane (the neighbouring regions own their other bytes)
+        const unsigned long long gend = g0 + wtot;
+        const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);  // first whole chunk
+        const uint32_t c1 = (uint32_t)((gend - ga) >> 4);        // end of the whole chunks
+        for (uint32_t c = c0 + lane; c < c1; c += 32u) {
+          const uint32_t w = c << 2;
+          uint4 v;
+          v.x = stg[stg_pad(w)];
+          v.y = stg[stg_pad(w + 1)];
+          v.z = stg[stg_pad(w + 2)];
+          v.w = stg[stg_pad(w + 3)];
+          *reinterpret_cast<uint4*>(p.out + ga + ((unsigned long long)c << 4)) = v;
+        }
+        {
+          // head bytes [g0, ga + 16*c0) on lanes 0-15, tail bytes [ga + 16*c1, gend) on 16-31;
+          // with no whole chunk, the region (< 32 bytes) is covered by all 32 lanes
+          unsigned long long b;
+          bool ok;
+          if (c0 < c1) {
+            b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
+            ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
           } else {
-            const uint32_t b0 = lo > sh ? lo : sh, b1 = hi < total ? hi : total;
-            for (uint32_t b = b0; b < b1; ++b) p.out[base_g + b] = sbytes[stg_pad(b >> 2) * 4u + (b & 3u)];
+            b = g0 + lane;
+            ok = b < gend;
+          }
+          if (ok) {
+            const uint32_t sbi = (uint32_t)(b - ga);
+            p.out[b] = sbytes[stg_pad(sbi >> 2) * 4u + (sbi & 3u)];
           }
         }
       } else if (fits && !failed) {
-        // very large expansions: windows of the output, byte by byte
+        // very large expansions: windows of the sub-tile output, byte by byte
+        const uint32_t ooff = wbase + toff;
+        const uint32_t sub_olen = sub_total;
         for (uint32_t w0 = 0; w0 < sub_olen; w0 += kOutWin) {
           const uint32_t w1 = (w0 + kOutWin) < sub_olen ? (w0 + kOutWin) : sub_olen;
           const unsigned long long g0 = O + w0;
@@ -1848,7 +2019,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           __syncthreads();
         }
       }
-      O += sub_olen;
+      O += sub_total;
       __syncthreads();
       ring.release();
       if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
@@ -1870,10 +2041,9 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         }
       }
     }
-    // advance the queue
+    // claim the next super-tile only now, when its pass A starts: a super-tile claimed
+    // early but started late would hold up the look-back of every later super-tile
     if (tid == 0) {
-      // claim the next super-tile only now, when its pass A starts: a super-tile claimed
-      // early but started late would hold up the look-back of every later super-tile
       const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
       s_q[0] = nx < NT ? nx : NT;
       s_q[1] = 0xFFFFFFFFu;
