@@ -38,6 +38,7 @@ using crb::ReplaceParams;
 using crb::TileIncl;
 
 constexpr int kErrUnknown = 999;  // cudaErrorUnknown
+constexpr int kFallback = -100;   // internal: the fast path does not apply, use the general one
 constexpr size_t kAllocQuantum = 2ull << 20;
 
 size_t round_up(size_t x, size_t q) { return (x + q - 1) / q * q; }
@@ -135,6 +136,9 @@ struct Session {
   unsigned long long launches = 0;
   unsigned long long kept_last = 0;
 
+  unsigned long long* lens = nullptr;       // device: lengths along an apply_batch chain
+  unsigned long long* lens_host = nullptr;  // page-locked mirror
+  size_t lens_cap = 0;
   cudaStream_t async_stream = nullptr;  // stream of the last cuda_replace_apply_device_async
   uint32_t async_epoch = 0;
 
@@ -256,6 +260,8 @@ void session_free(Session* s) {
   if (s->res_host) cudaFreeHost(s->res_host);
   if (s->ext) cudaFree(s->ext);
   if (s->ext_host) cudaFreeHost(s->ext_host);
+  if (s->lens) cudaFree(s->lens);
+  if (s->lens_host) cudaFreeHost(s->lens_host);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -459,6 +465,106 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
   return kErrUnknown;
 }
 
+// apply_batch with the lengths chained on the device: one launch per pair and a single
+// read-back at the end, instead of a host round trip per pair. Used when every pair runs on
+// the super-tile kernel with inline pattern bytes and the worst-case lengths along the chain
+// fit in memory; returns kFallback when the caller must use one apply per pair.
+int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+                        const int* rep_lens, int count, size_t* new_len) {
+  if (count <= 0 || !pats || !reps || !pat_lens || !rep_lens) return kFallback;
+  std::vector<ReplaceParams> ps((size_t)count);
+  size_t b = s->len, maxb = s->len, tiles_max = 1, entries_max = 1;
+  for (int k = 0; k < count; ++k) {
+    const int pl = pat_lens[k], rl = rep_lens[k];
+    if (pl < 1 || rl < 0 || pl > crb::kInlineMax || rl > crb::kInlineMax || !pats[k] || (rl && !reps[k])) return kFallback;
+    ReplaceParams& p = ps[(size_t)k];
+    memset(&p, 0, sizeof(p));
+    crb::prepare_pattern_fields(p, pats[k], (uint32_t)pl);
+    p.R = (uint32_t)rl;
+    p.nsub = crb::super_nsub(p.mode, p.L);
+    if (!p.nsub) return kFallback;
+    memcpy(p.pat, pats[k], (size_t)pl);
+    if (rl) memcpy(p.rep, reps[k], (size_t)rl);
+    const size_t tb = (size_t)crb::kTile * p.nsub;
+    const size_t tiles = (b + tb - 1) / tb;
+    p.num_tiles = (uint32_t)(tiles ? tiles : 1);
+    tiles_max = std::max(tiles_max, (size_t)p.num_tiles);
+    entries_max = std::max(entries_max, (size_t)p.num_tiles * p.agg_entries);
+    b = output_bound(b, p.L, p.R);
+    if (b == SIZE_MAX) return kFallback;
+    maxb = std::max(maxb, b);
+  }
+  if (maxb > std::max<size_t>(4 * s->len, s->len + (1ull << 30))) return kFallback;
+  cudaError_t e = dev_grow(&s->buf, &s->buf_cap, maxb ? maxb : 1, true, s->len, s->stream);
+  if (e == cudaSuccess) e = dev_grow(&s->alt, &s->alt_cap, maxb ? maxb : 1, false, 0, s->stream);
+  if (e == cudaSuccess) e = ensure_scratch(s, tiles_max, entries_max);
+  if (e != cudaSuccess) return (int)e;
+  if ((size_t)count + 1 > s->lens_cap) {
+    if (s->lens) cudaFree(s->lens);
+    if (s->lens_host) cudaFreeHost(s->lens_host);
+    s->lens = nullptr;
+    s->lens_host = nullptr;
+    const size_t cap = (size_t)count + 64;
+    e = cudaMalloc(&s->lens, cap * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->lens_host, cap * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+      s->lens_cap = 0;
+      return (int)e;
+    }
+    s->lens_cap = cap;
+  }
+  e = cudaStreamSynchronize(s->stream);  // the page-locked mirror may feed an earlier copy
+  if (e != cudaSuccess) return (int)e;
+  s->lens_host[0] = s->len;
+  e = cudaMemcpyAsync(s->lens, s->lens_host, sizeof(unsigned long long), cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) return (int)e;
+  uint8_t* bufs[2] = {s->buf, s->alt};
+  const size_t cap = std::min(s->buf_cap, s->alt_cap);
+  uint32_t first_epoch = 0;
+  for (int k = 0; k < count; ++k) {
+    ReplaceParams& p = ps[(size_t)k];
+    p.in = bufs[k & 1];
+    p.out = bufs[(k + 1) & 1];
+    p.n_dev = s->lens + k;
+    p.len_out = s->lens + k + 1;
+    p.out_cap = cap;
+    p.status = s->status;
+    p.incl = s->incl;
+    p.agg = s->agg;
+    p.res = s->res;
+    p.tile_last = s->tile_last;
+    p.rec = s->rec;
+    p.epoch = next_epoch(s);
+    if (k == 0) first_epoch = p.epoch;
+    e = crb::launch_replace_super(p, s->stream, nullptr);
+    if (e != cudaSuccess) return (int)e;
+    ++s->launches;
+  }
+  e = cudaMemcpyAsync(s->lens_host, s->lens, ((size_t)count + 1) * sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return (int)e;
+  const ApplyResult r = *s->res_host;
+  const uint32_t last_epoch = ps[(size_t)count - 1].epoch;
+  if ((r.error_epoch >= first_epoch && r.error_epoch <= last_epoch) ||
+      (r.overflow_epoch >= first_epoch && r.overflow_epoch <= last_epoch))
+    return kErrUnknown;
+  if (count & 1) swap_buffers(s);
+  s->len = (size_t)s->lens_host[count];
+  ReplaceParams q = ps[(size_t)count - 1];
+  q.n = s->lens_host[count - 1];
+  q.n_dev = nullptr;
+  q.len_out = nullptr;
+  s->q_kind = 2;
+  s->q_n = q.n;
+  s->q_params = q;
+  s->kept_last = r.kept;
+  if (new_len) *new_len = s->len;
+  return 0;
+}
+
 int query_prefix64(Session* s, size_t limit, long long* kept, long long* last) {
   *kept = 0;
   *last = -1;
@@ -645,6 +751,10 @@ CR_EXPORT int cuda_replace_query_prefix64(void* h, size_t limit, long long* kept
 CR_EXPORT int cuda_replace_apply_batch(void* h, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
                                        const int* rep_lens, int count, size_t* new_len) {
   SESSION_GUARD(h);
+  if (count > 1) {
+    const int rc = apply_batch_chained(s, pats, pat_lens, reps, rep_lens, count, new_len);
+    if (rc != kFallback) return rc;
+  }
   for (int i = 0; i < count; ++i) {
     const uint8_t* p = pats ? pats[i] : nullptr;
     const uint8_t* r = reps ? reps[i] : nullptr;

@@ -1147,7 +1147,7 @@ __device__ __forceinline__ unsigned long long rec_data(unsigned long long w) { r
 // tile with zero payload). Returns the nearest inclusive lane (32 if none) once every
 // nearer lane holds a valid record, or -1 when the wait gave up; d0/d1 receive the payload.
 __device__ __forceinline__ int warp_read_window(const ReplaceParams& p, long long base, unsigned long long* d0,
-                                                unsigned long long* d1) {
+                                                unsigned long long* d1, uint32_t carry0) {
   const uint32_t lane = threadIdx.x & 31u;
   const long long j = base - (long long)lane;
   const uint32_t tag = p.epoch & 0xFFFFFFu;
@@ -1158,6 +1158,7 @@ __device__ __forceinline__ int warp_read_window(const ReplaceParams& p, long lon
     unsigned long long w0 = 0, w1 = 0;
     if (j < 0) {
       st = kStInc;
+      w1 = carry0;  // the virtual tile before tile 0 leaves carry0 bytes covered
     } else {
       rec_load(p.rec, (uint32_t)j, &w0, &w1);
       const uint32_t s0 = (uint32_t)(w0 >> 38) & 3u, s1 = (uint32_t)(w1 >> 38) & 3u;
@@ -1186,7 +1187,7 @@ __device__ __forceinline__ int warp_read_window(const ReplaceParams& p, long lon
 }
 
 __device__ __forceinline__ bool lookback_free_rec(const ReplaceParams& p, uint32_t t, unsigned long long S,
-                                                  unsigned long long* K_out, uint32_t* c_out) {
+                                                  unsigned long long* K_out, uint32_t* c_out, uint32_t carry0) {
   const uint32_t lane = threadIdx.x & 31u;
   unsigned long long acc_cnt = 0;
   long long acc_cover = 0;
@@ -1194,7 +1195,7 @@ __device__ __forceinline__ bool lookback_free_rec(const ReplaceParams& p, uint32
   long long base = (long long)t - 1;
   for (;;) {
     unsigned long long d0, d1;
-    const int plr = warp_read_window(p, base, &d0, &d1);
+    const int plr = warp_read_window(p, base, &d0, &d1, carry0);
     if (plr < 0) return false;
     const uint32_t pl = (uint32_t)plr;
     unsigned long long cnt = 0;
@@ -1231,14 +1232,14 @@ __device__ __forceinline__ uint32_t tab4_entry(unsigned long long d0, unsigned l
 }
 
 __device__ __forceinline__ bool lookback_small4_rec(const ReplaceParams& p, uint32_t t, uint32_t L,
-                                                    unsigned long long* K_out, uint32_t* c_out) {
+                                                    unsigned long long* K_out, uint32_t* c_out, uint32_t carry0) {
   const uint32_t lane = threadIdx.x & 31u;
   unsigned long long acc_cnt = 0;  // lane c < L: function of the tiles between the window and t
   uint32_t acc_carry = lane;
   long long base = (long long)t - 1;
   for (;;) {
     unsigned long long d0, d1;
-    const int plr = warp_read_window(p, base, &d0, &d1);
+    const int plr = warp_read_window(p, base, &d0, &d1, carry0);
     if (plr < 0) return false;
     const uint32_t pl = (uint32_t)plr;
     if (pl < 32) {
@@ -1279,7 +1280,7 @@ __device__ __forceinline__ bool lookback_small4_rec(const ReplaceParams& p, uint
 // Mode small (L <= 32): tile functions are tables over carries; lane c holds entry c.
 // acc is the function of the tiles between the current window and t.
 __device__ __forceinline__ bool lookback_small(const ReplaceParams& p, uint32_t t, uint32_t L,
-                                               unsigned long long* K_out, uint32_t* c_out) {
+                                               unsigned long long* K_out, uint32_t* c_out, uint32_t carry0) {
   const uint32_t lane = threadIdx.x & 31u;
   unsigned long long acc_cnt = 0;
   uint32_t acc_carry = lane;
@@ -1300,7 +1301,7 @@ __device__ __forceinline__ bool lookback_small(const ReplaceParams& p, uint32_t 
     }
     if (pl < 32) {
       unsigned long long K = 0;
-      uint32_t x = 0;
+      uint32_t x = carry0;
       const long long jp = base - (long long)pl;
       if (jp >= 0) {
         K = __ldcg(&p.incl[jp].kept);
@@ -1456,13 +1457,13 @@ struct LoadRing {
   }
   __device__ __forceinline__ void issue(const ReplaceParams& p, uint8_t* smem, const LayoutS& lay,
                                         uint64_t* bars, uint32_t* q, unsigned long long S,
-                                        unsigned long long n16, uint32_t want_a) {
-    const uint32_t NT = p.num_tiles;
+                                        unsigned long long n16, uint32_t want_a, unsigned long long n,
+                                        uint32_t NT) {
     while (issued - consumed < (uint32_t)kNBuf) {
       if (iq >= 1) break;  // loads of the next super-tile start once it is claimed
       const uint32_t tile = q[iq];
       if (tile >= NT) break;
-      const uint32_t m = subs_in_tile(tile, S, p.n, p.nsub);
+      const uint32_t m = subs_in_tile(tile, S, n, p.nsub);
       const unsigned long long start = (unsigned long long)tile * S + (unsigned long long)ij * kTile;
       const unsigned long long avail = n16 - start;
       const uint32_t want = iph == 0 ? want_a : (uint32_t)kTile;
@@ -1521,11 +1522,20 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   uint64_t* masks = reinterpret_cast<uint64_t*>(smem + lay.masks);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t sb = tid * kSeg;
-  const unsigned long long n = p.n;
-  const unsigned long long n16 = (n + 15ull) & ~15ull;
+  // n_all bytes are in the buffer (matches may reach up to it); output covers the first n
+  const unsigned long long n_all = p.n_dev ? *p.n_dev : p.n;
+  const unsigned long long n = n_all > p.hold ? n_all - p.hold : 0ull;
+  const unsigned long long n16 = (n_all + 15ull) & ~15ull;
   const unsigned long long S = (unsigned long long)nsub * kTile;
   const uint32_t want_a = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16);
-  const uint32_t NT = p.num_tiles;
+  const uint32_t NT = (uint32_t)min((n + S - 1ull) / S, (unsigned long long)p.num_tiles);
+  const uint32_t carry0 = p.carry0_dev ? *p.carry0_dev : p.carry0;
+  if (NT == 0 && blockIdx.x == 0 && threadIdx.x == 0) {  // nothing to emit: still report
+    if (p.len_out) *p.len_out = 0ull;
+    if (p.carry_out) *p.carry_out = carry0 > n ? carry0 - (uint32_t)n : 0u;
+    p.res->out_len = 0;
+    p.res->kept = 0;
+  }
   const bool warp_stage = R <= 3u * L;  // every warp's output fits its staging area
 
   {
@@ -1558,7 +1568,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     s_fail = 0;
   }
   __syncthreads();
-  if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+  if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
 
   for (;;) {
     __syncthreads();
@@ -1580,8 +1590,9 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           const unsigned long long d = p.block_before - gseg;
           lo = d < 64ull ? (uint32_t)d : 64u;
         }
-        if (n >= L && n - L + 1 > gseg) {
-          const unsigned long long d = n - L + 1 - gseg;
+        const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
+        if (lim > gseg) {
+          const unsigned long long d = lim - gseg;
           hi = d < 64ull ? (uint32_t)d : 64u;
         }
         mask &= low_bits(hi) & ~low_bits(lo);
@@ -1634,7 +1645,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       }
       __syncthreads();
       ring.release();
-      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
     }
 
     // ================= fold the sub-tiles into the super-tile function
@@ -1698,15 +1709,15 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     // ================= look back, publish the inclusive prefix
     if (warp == 0) {
       unsigned long long K = 0;
-      uint32_t c = 0;
+      uint32_t c = carry0;
       bool ok = true;
       if (t > 0) {
         if (MODE == kModeFree)
-          ok = lookback_free_rec(p, t, S, &K, &c);
+          ok = lookback_free_rec(p, t, S, &K, &c, carry0);
         else if (use_rec)
-          ok = lookback_small4_rec(p, t, L, &K, &c);
+          ok = lookback_small4_rec(p, t, L, &K, &c, carry0);
         else
-          ok = lookback_small(p, t, L, &K, &c);
+          ok = lookback_small(p, t, L, &K, &c, carry0);
       }
       if (!ok) {
         K = 0;
@@ -1718,7 +1729,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       if (MODE == kModeFree) {
         const unsigned long long fcnt = __shfl_sync(0xffffffffu, fr_cnt, 0);
         const long long flco = __shfl_sync(0xffffffffu, fr_lco, 0);
-        const long long sh = (long long)c - (long long)S;
+        const long long sh = (long long)c - (long long)m * kTile;  // span of this super-tile
         const long long co = sh > flco ? sh : flco;
         Kin = K + fcnt;
         cout = co > 0 ? (uint32_t)co : 0u;
@@ -2022,7 +2033,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       O += sub_total;
       __syncthreads();
       ring.release();
-      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
     }
 
     // ================= per-super-tile records: last kept start, totals
@@ -2038,6 +2049,13 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         if (t == NT - 1) {
           p.res->out_len = O;
           p.res->kept = __ldcg(&p.incl[t].kept);
+          if (p.len_out) *p.len_out = O;
+          if (p.carry_out) {
+            // coverage past the output range n: the inclusive carry minus the tile's unused span
+            const unsigned long long tail = tstart + (unsigned long long)m * kTile - n;  // bytes of the last tile past n
+            const unsigned int ci = __ldcg(&p.incl[t].carry);
+            *p.carry_out = (unsigned long long)ci + tail;
+          }
         }
       }
     }
@@ -2049,7 +2067,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       s_q[1] = 0xFFFFFFFFu;
       ring.shift();
       s_fail = 0;
-      ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a);
+      ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
     }
   }
 

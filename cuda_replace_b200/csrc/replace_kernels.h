@@ -81,6 +81,20 @@ struct ReplaceParams {
   ApplyResult* res;
   long long* tile_last;           // super-tile kernel: last kept start per super-tile or -1 [num_tiles]
   unsigned long long* rec;        // super-tile kernel: 16-byte look-back record per super-tile [2 * num_tiles]
+  // Chaining (super-tile kernel). When n_dev is set the input length is read from device
+  // memory (the previous launch's len_out), so launches chain without a host round trip;
+  // num_tiles is then only an upper bound. `hold` trailing bytes are matched against but
+  // produce no output (a streaming chunk keeps them for the next chunk). carry0 (or
+  // *carry0_dev) leading bytes are covered by a match kept before this buffer; the last
+  // tile writes the output length to *len_out and the coverage past the output range to
+  // *carry_out.
+  const unsigned long long* n_dev;
+  unsigned long long* len_out;
+  const unsigned int* carry0_dev;
+  unsigned int* carry_out;
+  unsigned long long hold;
+  unsigned int carry0;
+  unsigned int pad1;
   const uint8_t* pat_ext;         // device copy when L > kInlineMax
   const uint8_t* rep_ext;         // device copy when R > kInlineMax
   uint8_t pat[kInlineMax];

@@ -194,3 +194,31 @@ def test_launch_counter_counts_kernels(cr_lib):
         s.apply(b"b", b"cc")
         kept, l1 = s.stats()
         assert l1 - l0 == 2 and kept == 50000
+
+
+def test_apply_batch_chained_matches_pairwise(cr_lib, oracle_mod):
+    """apply_batch chains lengths on the device (no host round trip per pair); the result,
+    the final length and the following query_prefix must equal the pair-by-pair chain."""
+    rng = random.Random(31)
+    base = WL.text_corpus(600_000, seed=7)
+    for trial in range(6):
+        pairs = []
+        for _ in range(rng.choice([2, 3, 7, 16])):
+            w = rng.choice([b"aa", b"a", b"ab", b"the", b"e ", b"&amp;", b"xyz", b"\n", b"ss"])
+            rep = bytes(rng.choice(b"QRS") for _ in range(rng.randint(0, 5)))
+            pairs.append((w, rep))
+        src = base[: rng.randint(1, len(base))]
+        exp = src
+        for p_, r_ in pairs:
+            exp = exp.replace(p_, r_)
+        with Wr.Session(cr_lib, src) as s:
+            n = s.apply_batch(pairs)
+            assert n == len(exp) and s.length() == len(exp)
+            assert s.result() == exp
+            # query_prefix describes the last pair applied to the second-to-last output
+            prev = src
+            for p_, r_ in pairs[:-1]:
+                prev = prev.replace(p_, r_)
+            lp = pairs[-1][0]
+            for lim in (0, len(prev) // 3, len(prev)):
+                assert s.query_prefix(lim) == oracle_mod.query_prefix(prev, lp, lim), (trial, lim)
