@@ -17,7 +17,7 @@ REPO_DIR = PKG_DIR.parent
 CSRC = PKG_DIR / "csrc"
 LIB_NAME = "libcuda_replace.so"
 LIB_PATH = PKG_DIR / LIB_NAME
-SOURCES = ["replace_kernels.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["replace_kernels.cu", "capi.cu", "noalloc.cu", "stream.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -36,7 +36,7 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 
 def build(force: bool = False, ptxas_verbose: bool = False) -> Path:
-    deps = [CSRC / s for s in SOURCES] + [CSRC / "replace_kernels.h", REPO_DIR / "include" / "cuda_replace.h"]
+    deps = [CSRC / s for s in SOURCES] + [CSRC / "replace_kernels.h", CSRC / "host_pool.h", REPO_DIR / "include" / "cuda_replace.h"]
     if not force and not ptxas_verbose and not _stale(LIB_PATH, deps):
         return LIB_PATH
     tmp = LIB_PATH.with_suffix(".so.tmp")

@@ -827,6 +827,17 @@ __global__ void __launch_bounds__(kThreads) query_tile_kernel(const __grid_const
   }
 }
 
+// ============================================================================ held tail
+// Streaming: copy the last P bytes of buf[0, min(*total, cap)) to dst, where *total is the
+// length a previous launch left in device memory. Bytes before position 0 read as zero.
+__global__ void move_tail_kernel(const uint8_t* __restrict__ buf, const unsigned long long* __restrict__ total,
+                                 unsigned long long cap, uint32_t P, uint8_t* __restrict__ dst) {
+  unsigned long long t = *total;
+  if (t > cap) t = cap;
+  const unsigned long long from = t >= P ? t - P : 0ull;
+  for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) dst[i] = (from + i < t) ? buf[from + i] : (uint8_t)0;
+}
+
 // ============================================================================ empty pattern
 // bytes.replace(b"", rep): rep before every input byte and once at the end.
 __global__ void empty_pattern_kernel(const uint8_t* __restrict__ in, unsigned long long n,
@@ -1523,7 +1534,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t sb = tid * kSeg;
   // n_all bytes are in the buffer (matches may reach up to it); output covers the first n
-  const unsigned long long n_all = p.n_dev ? *p.n_dev : p.n;
+  const unsigned long long n_all = p.n_dev ? min(*p.n_dev, p.n_cap ? p.n_cap : ~0ull) : p.n;
   const unsigned long long n = n_all > p.hold ? n_all - p.hold : 0ull;
   const unsigned long long n16 = (n_all + 15ull) & ~15ull;
   const unsigned long long S = (unsigned long long)nsub * kTile;
@@ -1531,7 +1542,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   const uint32_t NT = (uint32_t)min((n + S - 1ull) / S, (unsigned long long)p.num_tiles);
   const uint32_t carry0 = p.carry0_dev ? *p.carry0_dev : p.carry0;
   if (NT == 0 && blockIdx.x == 0 && threadIdx.x == 0) {  // nothing to emit: still report
-    if (p.len_out) *p.len_out = 0ull;
+    if (p.len_out) *p.len_out = p.len_bias;
     if (p.carry_out) *p.carry_out = carry0 > n ? carry0 - (uint32_t)n : 0u;
     p.res->out_len = 0;
     p.res->kept = 0;
@@ -1753,7 +1764,9 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     const uint32_t cin = s_cin;
     const unsigned long long kexcl = s_kexcl;
     const long long delta = (long long)R - (long long)L;
-    unsigned long long O = (unsigned long long)((long long)(tstart + cin) + (long long)kexcl * delta);
+    // output position in out[]: the output range starts len_bias bytes in
+    unsigned long long O =
+        p.len_bias + (unsigned long long)((long long)(tstart + cin) + (long long)kexcl * delta);
     const bool failed = s_fail != 0;
 
     // ================= pass B: exact kept starts and output, one warp region at a time
@@ -2047,7 +2060,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
         if (lastt >= 0)
           atomicMax(&p.res->last_tagged, ((unsigned long long)p.epoch << 40) | (unsigned long long)(lastt + 1));
         if (t == NT - 1) {
-          p.res->out_len = O;
+          p.res->out_len = O - p.len_bias;
           p.res->kept = __ldcg(&p.incl[t].kept);
           if (p.len_out) *p.len_out = O;
           if (p.carry_out) {
@@ -2370,6 +2383,12 @@ cudaError_t launch_query(const ReplaceParams& p, cudaStream_t st) {
     case kModeSmall: query_tile_kernel<kModeSmall><<<1, kThreads, smem, st>>>(p); break;
     default: query_tile_kernel<kModeLarge><<<1, kThreads, smem, st>>>(p); break;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_move_tail(const uint8_t* buf, const unsigned long long* total, unsigned long long cap,
+                             uint32_t P, uint8_t* dst, cudaStream_t st) {
+  move_tail_kernel<<<1, 256, 0, st>>>(buf, total, cap, P, dst);
   return cudaGetLastError();
 }
 

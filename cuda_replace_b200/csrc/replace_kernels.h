@@ -93,6 +93,9 @@ struct ReplaceParams {
   const unsigned int* carry0_dev;
   unsigned int* carry_out;
   unsigned long long hold;
+  unsigned long long n_cap;       // with n_dev: the input buffer's capacity (a longer length is clamped)
+  unsigned long long len_bias;    // output starts this many bytes into out (out stays 16-byte aligned);
+                                  // *len_out receives len_bias + the output length
   unsigned int carry0;
   unsigned int pad1;
   const uint8_t* pat_ext;         // device copy when L > kInlineMax
@@ -117,6 +120,9 @@ cudaError_t launch_query_super(const ReplaceParams& p, cudaStream_t st);
 // One CTA answers query_prefix for tile p.query_tile at tile-relative limit p.query_limit,
 // using the tile records of the apply described by p; writes res->q_kept / res->q_last.
 cudaError_t launch_query(const ReplaceParams& p, cudaStream_t st);
+// Copy the last P bytes of buf[0, min(*total, cap)) to dst (streaming: a stage's held tail).
+cudaError_t launch_move_tail(const uint8_t* buf, const unsigned long long* total, unsigned long long cap,
+                             uint32_t P, uint8_t* dst, cudaStream_t st);
 // bytes.replace with an empty pattern: rep before every byte and at the end.
 cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const uint8_t* rep_dev,
                                  uint32_t R, uint8_t* out, cudaStream_t st);

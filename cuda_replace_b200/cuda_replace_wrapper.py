@@ -80,6 +80,9 @@ class CudaReplaceLib:
               C.c_int, optional=True)
         _bind(lib, "cuda_replace_device_result", [c_void_p, c_size_t_p, C.POINTER(C.c_ulonglong)], C.c_int,
               optional=True)
+        _bind(lib, "cuda_replace_stream",
+              [c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t,
+               C.POINTER(c_uint8_p), c_size_t_p], C.c_int, optional=True)
 
     def version(self) -> str:
         return self.lib.cuda_replace_version().decode()
@@ -250,14 +253,98 @@ def stream_chunk_plan(n: int, chunk_bytes: int) -> List[Tuple[int, int]]:
     return [(p, min(p + chunk_bytes, n)) for p in range(0, n, chunk_bytes)]
 
 
+STREAM_UNSUPPORTED = -7  # cuda_replace_stream: a pair outside its limits
+
+
+def _pair_arrays(pairs: Sequence[Tuple[bytes, bytes]]):
+    count = max(len(pairs), 1)
+    keep = []
+    pat_ptrs = (c_uint8_p * count)()
+    rep_ptrs = (c_uint8_p * count)()
+    pat_lens = (C.c_int * count)()
+    rep_lens = (C.c_int * count)()
+    for i, (pat, rep) in enumerate(pairs):
+        pb = C.create_string_buffer(pat, len(pat) or 1)
+        rb = C.create_string_buffer(rep, len(rep) or 1)
+        keep += [pb, rb]
+        pat_ptrs[i] = C.cast(pb, c_uint8_p)
+        rep_ptrs[i] = C.cast(rb, c_uint8_p)
+        pat_lens[i] = len(pat)
+        rep_lens[i] = len(rep)
+    return keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens
+
+
+def stream_native(lib: CudaReplaceLib, src, pairs: Sequence[Tuple[bytes, bytes]],
+                  chunk_bytes: int) -> Optional[bytes]:
+    """Chunk-major streaming through cuda_replace_stream: every pair is applied to a chunk on
+    the device before the next chunk is read. None when the library lacks the entry point or
+    a pair is outside its limits (pattern 1-256 bytes, bordered patterns up to 32 bytes,
+    replacement up to 256 bytes)."""
+    fn = getattr(lib.lib, "cuda_replace_stream", None)
+    if fn is None:
+        return None
+    keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(pairs)
+    mv = memoryview(src)
+    n = mv.nbytes
+    if not n:
+        holder, src_ptr = None, c_uint8_p()
+    elif isinstance(src, bytes) or mv.readonly:
+        holder = src if isinstance(src, bytes) else bytes(mv)
+        src_ptr = C.cast(C.c_char_p(holder), c_uint8_p)  # points into the bytes object: no copy
+    else:
+        holder = (C.c_uint8 * n).from_buffer(mv)
+        src_ptr = C.cast(holder, c_uint8_p)
+    out_ptr = c_uint8_p()
+    out_len = c_size_t()
+    rc = fn(src_ptr, c_size_t(n), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
+            C.cast(rep_ptrs, c_uint8_pp), C.cast(rep_lens, c_int_p), C.c_int(len(pairs)),
+            c_size_t(int(chunk_bytes)), C.byref(out_ptr), C.byref(out_len))
+    del keep, holder
+    if rc == STREAM_UNSUPPORTED:
+        return None
+    if rc != 0:
+        raise RuntimeError(f"cuda_replace_stream failed rc={rc}")
+    try:
+        return C.string_at(out_ptr, out_len.value) if out_len.value else b""
+    finally:
+        lib.lib.cuda_free_host(out_ptr)
+
+
+def _stream_supported(lib: CudaReplaceLib, pat: bytes, rep: bytes) -> bool:
+    """Whether cuda_replace_stream takes this pair (asked with an empty input)."""
+    return getattr(lib.lib, "cuda_replace_stream", None) is not None and \
+        stream_native(lib, b"", [(pat, rep)], 1) is not None
+
+
 def gpu_replace_streaming(lib: CudaReplaceLib, src: bytes, pairs: Iterable[Tuple[bytes, bytes]],
                           chunk_bytes: int = 256 * 1024 * 1024) -> bytes:
-    """Chunked, pair-major replacement of an input larger than device memory
-    (reference signature: py:305-308). Each chunk carries an (L-1)-byte halo; the carry-in
-    is the start of the previous chunk's last kept match, passed to apply_seeded."""
+    """Chunked replacement of an input larger than device memory (reference signature:
+    py:305-308). Runs of consecutive pairs that cuda_replace_stream takes go through it
+    chunk-major; any other pair is streamed pair-major: each chunk carries an (L-1)-byte
+    halo, and the carry-in is the start of the previous chunk's last kept match, passed to
+    apply_seeded."""
+    pairs = list(pairs)
+    out = src
+    i = 0
+    while i < len(pairs):
+        j = i
+        while j < len(pairs) and _stream_supported(lib, *pairs[j]):
+            j += 1
+        if j > i:
+            res = stream_native(lib, out, pairs[i:j], chunk_bytes)
+            if res is None:
+                raise RuntimeError("cuda_replace_stream rejected pairs it accepted alone")
+            out, i = res, j
+        else:
+            out = _stream_pair_major(lib, out, pairs[i], chunk_bytes)
+            i += 1
+    return out
+
+
+def _stream_pair_major(lib: CudaReplaceLib, src: bytes, pair: Tuple[bytes, bytes], chunk_bytes: int) -> bytes:
     out = src
     with Session(lib, b"") as sess:
-        for pat, rep in pairs:
+        for pat, rep in [pair]:
             L = len(pat)
             n = len(out)
             pieces: List[bytes] = []

@@ -18,6 +18,7 @@
  *   -5   a 32-bit output of cuda_replace_query_prefix cannot hold the value
  *        (use cuda_replace_query_prefix64)
  *   -6   a size above the fixed limits of cuda_replace_apply_device_noalloc
+ *   -7   cuda_replace_stream: a pair outside the limits of the chunk-major path
  *   >0   a cudaError_t; 999 (cudaErrorUnknown) for internal failures, including a
  *        bounded device-side wait that gave up
  *
@@ -162,6 +163,24 @@ int cuda_replace_apply_device_noalloc(const uint8_t* d_in, size_t n,
                                       const uint8_t* rep, int rep_len,
                                       uint8_t* d_out, size_t out_cap, size_t* out_len,
                                       void* stream);
+
+/* Chunk-major streaming: apply every (pats[k], reps[k]) in order, as chained bytes.replace,
+ * to src[0, n), read chunk_bytes at a time (0 = 256 MiB), so n may exceed device memory.
+ * Replaces the pair-major helper gpu_replace_streaming (cuda_replace_wrapper.py:305-366),
+ * which crosses the host link twice per pair and drops the replacement of a match that
+ * straddles a chunk boundary (py:356); here the result equals chained bytes.replace for any
+ * chunk size. Each chunk passes through all pairs on the device before the next chunk is
+ * needed: each pair holds its last pat_len - 1 bytes back for the next chunk, the coverage of
+ * a match kept before a chunk is carried into it, lengths between pairs stay on the device,
+ * and the next chunk's upload and the previous chunk's download overlap the compute.
+ * *out_host receives page-locked memory to release with cuda_free_host (NULL when the result
+ * is empty). Limits: pat_lens in [1, 256], rep_lens in [0, 256], and a pattern with a proper
+ * border (a prefix that is also a suffix) at most 32 bytes long; -7 when a pair is outside
+ * them (stream such pairs pair-major); -1 for NULL arguments or a negative length;
+ * >0 a cudaError_t. */
+int cuda_replace_stream(const uint8_t* src, size_t n, const uint8_t** pats, const int* pat_lens,
+                        const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
+                        uint8_t** out_host, size_t* out_len);
 
 #ifdef __cplusplus
 }

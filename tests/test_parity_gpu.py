@@ -222,3 +222,59 @@ def test_apply_batch_chained_matches_pairwise(cr_lib, oracle_mod):
             lp = pairs[-1][0]
             for lim in (0, len(prev) // 3, len(prev)):
                 assert s.query_prefix(lim) == oracle_mod.query_prefix(prev, lp, lim), (trial, lim)
+
+
+def _native_stream(cr_lib, src, pairs, chunk):
+    out = Wr.stream_native(cr_lib, src, pairs, chunk)
+    assert out is not None, "cuda_replace_stream rejected a supported pair list"
+    return out
+
+
+@pytest.mark.parametrize("chunk", [1, 7, 16, 255, 4096, 16384 + 3, 1 << 20])
+def test_native_stream_small_chunks(cr_lib, chunk):
+    """Chunk-major streaming: every pair holds L-1 bytes back per chunk and carries match
+    coverage into the next chunk; the result must equal chained bytes.replace for any cut."""
+    rng = random.Random(chunk)
+    for trial in range(4):
+        base = rng.choice([b"a", b"ab", b"aab", b"abc"])
+        n = rng.choice([n for n in (1, 50, 5000, 70000) if n <= 400 * chunk])
+        src = bytearray((base * (n // len(base) + 1))[:n])
+        for _ in range(rng.randint(0, 30)):
+            src[rng.randrange(n)] = ord("z")
+        src = bytes(src)
+        pairs = []
+        for _ in range(rng.randint(1, 5)):
+            pat = (base * 8)[:rng.randint(1, 6)]
+            rep = bytes(rng.choice(b"abzQ") for _ in range(rng.randint(0, 5)))
+            pairs.append((pat, rep))
+        assert _native_stream(cr_lib, src, pairs, chunk) == chain(src, pairs), (chunk, trial, pairs)
+
+
+def test_native_stream_planted_straddles(cr_lib):
+    txt = WL.text_corpus(6 << 20, seed=9)
+    pairs = WL.c4_pairs(seed=9)
+    chunk = 1 << 20
+    for pat, _ in pairs[:4]:
+        txt, _count = WL.plant_across_boundaries(txt, pat, chunk, seed=len(pat) + 1)
+    exp = chain(txt, pairs)
+    assert _native_stream(cr_lib, txt, pairs, chunk) == exp
+    assert _native_stream(cr_lib, bytearray(txt), pairs, chunk) == exp
+    assert Wr.gpu_replace_streaming(cr_lib, txt, pairs, chunk_bytes=chunk) == exp
+
+
+def test_native_stream_expansion_regrows(cr_lib):
+    # outputs far above the planned capacity: stages overflow and the chunk runs again
+    src = b"a" * 3_000_000 + b"b" * 1000
+    pairs = [(b"a", b"Q" * 200), (b"QQ", b"RRR"), (b"b", b"")]
+    assert _native_stream(cr_lib, src, pairs, 1 << 20) == chain(src, pairs)
+
+
+def test_native_stream_limits_and_mixed_pairs(cr_lib):
+    assert Wr.stream_native(cr_lib, b"abc", [(b"", b"x")], 16) is None
+    assert Wr.stream_native(cr_lib, b"abc", [(b"ab" * 20, b"x")], 16) is None  # bordered, L > 32
+    assert Wr.stream_native(cr_lib, b"abc", [(b"a" * 300, b"x")], 16) is None
+    assert Wr.stream_native(cr_lib, b"", [(b"a", b"x")], 16) == b""
+    assert Wr.stream_native(cr_lib, b"abc", [], 16) == b"abc"
+    src = (b"ab" * 30000 + b"c") * 3
+    pairs = [(b"c", b"cc"), (b"ab" * 20, b"Z"), (b"", b"-"), (b"-Z", b"z"), (b"b-", b"")]
+    assert Wr.gpu_replace_streaming(cr_lib, src, pairs, chunk_bytes=10000) == chain(src, pairs)
