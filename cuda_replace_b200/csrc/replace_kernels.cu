@@ -1521,6 +1521,7 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   __shared__ unsigned long long s_kexcl;
   __shared__ uint32_t s_cin;
   __shared__ uint32_t s_fail;
+  __shared__ uint32_t s_cutlen;             // exact output length of the warp region cut at n
   __shared__ uint32_t s_sub_lco[kMaxSub];
   __shared__ uint32_t s_wcnt[kMaxSub * kWarps];   // kModeFree: kept count per (sub-tile, warp)
   __shared__ uint32_t s_wcend[kMaxSub * kWarps];  // kModeFree: max cover end per (sub-tile, warp)
@@ -1764,9 +1765,10 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     const uint32_t cin = s_cin;
     const unsigned long long kexcl = s_kexcl;
     const long long delta = (long long)R - (long long)L;
-    // output position in out[]: the output range starts len_bias bytes in
-    unsigned long long O =
-        p.len_bias + (unsigned long long)((long long)(tstart + cin) + (long long)kexcl * delta);
+    // output position in out[]: the output range starts len_bias bytes in, and the carry0
+    // leading bytes covered by a match kept before this buffer are not emitted here
+    unsigned long long O = p.len_bias + (unsigned long long)((long long)(tstart + cin) - (long long)carry0 +
+                                                             (long long)kexcl * delta);
     const bool failed = s_fail != 0;
 
     // ================= pass B: exact kept starts and output, one warp region at a time
@@ -1843,11 +1845,6 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           cnt = w.cnt;
         }
       }
-      uint32_t wbase, sub_total;
-      lanes8_sum(wolen, &wbase, &sub_total);
-      wbase = __shfl_sync(0xffffffffu, wbase, warp);
-      sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
-
       const uint32_t V = gseg >= n ? 0u : ((n - gseg) < 64ull ? (uint32_t)(n - gseg) : 64u);
       uint32_t covered = x_in < V ? x_in : V;
       if (cnt) {
@@ -1860,6 +1857,23 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
       uint32_t toff = warp_incl_scan(olen, OpSum());
       const uint32_t wtot = __shfl_sync(0xffffffffu, toff, 31);
       toff -= olen;  // exclusive offset inside the warp region
+
+      // The warp region that holds the end n of the output range is cut short. When input is
+      // held back past n, a match kept there may run beyond n, which the region functions
+      // (built over whole 2048-byte regions) do not see; the region's exact length is the sum
+      // over its threads. At most one sub-tile per launch has such a region; `cut` is the
+      // same in every warp (all compute the eight regions' lengths), so the barrier is uniform.
+      const uint32_t cut = __ballot_sync(0xffffffffu, lane < 8u && wbytes != 0u && wbytes < 2048u);
+      if (cut) {
+        const uint32_t cw = (uint32_t)__ffs(cut) - 1u;
+        if (warp == cw && lane == 0) s_cutlen = wtot;
+        __syncthreads();
+        if (lane == cw) wolen = s_cutlen;
+      }
+      uint32_t wbase, sub_total;
+      lanes8_sum(wolen, &wbase, &sub_total);
+      wbase = __shfl_sync(0xffffffffu, wbase, warp);
+      sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
 
       const bool fits = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
       if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
@@ -2064,10 +2078,11 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
           p.res->kept = __ldcg(&p.incl[t].kept);
           if (p.len_out) *p.len_out = O;
           if (p.carry_out) {
-            // coverage past the output range n: the inclusive carry minus the tile's unused span
-            const unsigned long long tail = tstart + (unsigned long long)m * kTile - n;  // bytes of the last tile past n
-            const unsigned int ci = __ldcg(&p.incl[t].carry);
-            *p.carry_out = (unsigned long long)ci + tail;
+            // coverage past the output range n: by the last kept match, or by the carry into
+            // this super-tile when no match starts in it
+            unsigned long long e = tstart + cin;
+            if (lastt >= 0 && (unsigned long long)lastt + L > e) e = (unsigned long long)lastt + L;
+            *p.carry_out = e > n ? (unsigned int)(e - n) : 0u;
           }
         }
       }

@@ -228,7 +228,7 @@ struct Stream {
   }
 
   // Enqueue every stage of one chunk (m new bytes in in0[b] after the P_0 held bytes).
-  cudaError_t run_chunk(int b, size_t m, bool final, uint32_t* first_epoch) {
+  cudaError_t run_chunk(int b, size_t m, bool first, bool final, uint32_t* first_epoch) {
     cudaError_t e = reserve_epochs((uint32_t)count);
     if (e != cudaSuccess) return e;
     *first_epoch = epoch + 1;
@@ -252,6 +252,9 @@ struct Stream {
       }
       p.num_tiles = (uint32_t)((in_cap + tile_bytes(k) - 1) / tile_bytes(k) + 1);
       p.hold = final ? 0 : s.P;
+      // At the first chunk the held bytes are placeholders: no match may start in them (the
+      // carry covers them too, but a pattern without a border keeps every occurrence it finds).
+      p.block_before = first ? s.P : 0;
       p.carry0_dev = carry + 2 * k + b;
       p.carry_out = carry + 2 * k + (b ^ 1);
       if (k + 1 < count) {
@@ -337,7 +340,10 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
     if (e == cudaSuccess && !src_pinned) S.hin[b] = static_cast<uint8_t*>(pool.get(S.chunk, &e));
   }
   for (int k = 0; k < count && e == cudaSuccess; ++k)
-    for (int b = 0; b < 2 && e == cudaSuccess; ++b) e = cudaMalloc(&S.st[(size_t)k].pend[b], 256);
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+      e = cudaMalloc(&S.st[(size_t)k].pend[b], 256);
+      if (e == cudaSuccess) e = cudaMemsetAsync(S.st[(size_t)k].pend[b], 0, 256, S.comp);
+    }
   if (e == cudaSuccess) e = cudaMalloc(&S.lens, (size_t)(count + 1) * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemsetAsync(S.lens, 0, (size_t)(count + 1) * sizeof(unsigned long long), S.comp);
   if (e == cudaSuccess) e = cudaMalloc(&S.outlen, 2 * sizeof(unsigned long long));
@@ -389,7 +395,7 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
     for (int attempt = 0;; ++attempt) {
       e = cudaStreamWaitEvent(S.comp, S.ev_h2d[b], 0);
       uint32_t e0 = 0;
-      if (e == cudaSuccess) e = S.run_chunk(b, m, final, &e0);
+      if (e == cudaSuccess) e = S.run_chunk(b, m, c == 0, final, &e0);
       if (e == cudaSuccess && attempt == 0 && !final) e = upload(c + 1);  // overlaps this chunk's stages
       if (e == cudaSuccess) e = cudaStreamSynchronize(S.comp);
       if (e != cudaSuccess) {
