@@ -31,6 +31,15 @@ c_size_t_p = C.POINTER(c_size_t)
 c_uint8_pp = C.POINTER(c_uint8_p)
 
 
+def _bytes_at(ptr, n: int) -> bytes:
+    """Copy n bytes of library-owned memory into a bytes object (ctypes.string_at takes a
+    C int size, which results of 2 GiB and more overflow)."""
+    if not n:
+        return b""
+    addr = C.cast(ptr, c_void_p).value
+    return memoryview((C.c_uint8 * n).from_address(addr)).cast("B").tobytes()
+
+
 def _bind(lib: C.CDLL, name: str, argtypes, restype, optional: bool = False) -> None:
     if optional and not hasattr(lib, name):
         setattr(lib, name, None)  # additive entry point absent from this build
@@ -102,7 +111,7 @@ class CudaReplaceLib:
         if rc != 0:
             raise RuntimeError(f"cuda_replace_unified failed rc={rc}")
         try:
-            return C.string_at(out_ptr, out_len.value) if out_len.value else b""
+            return _bytes_at(out_ptr, out_len.value)
         finally:
             self.lib.cuda_free_host(out_ptr)
 
@@ -199,7 +208,7 @@ class Session:
         if rc != 0:
             raise RuntimeError(f"cuda_replace_result failed rc={rc}")
         try:
-            return C.string_at(out_ptr, out_len.value) if out_len.value else b""
+            return _bytes_at(out_ptr, out_len.value)
         finally:
             self.lib.lib.cuda_free_host(out_ptr)
 
@@ -305,7 +314,7 @@ def stream_native(lib: CudaReplaceLib, src, pairs: Sequence[Tuple[bytes, bytes]]
     if rc != 0:
         raise RuntimeError(f"cuda_replace_stream failed rc={rc}")
     try:
-        return C.string_at(out_ptr, out_len.value) if out_len.value else b""
+        return _bytes_at(out_ptr, out_len.value)
     finally:
         lib.lib.cuda_free_host(out_ptr)
 
