@@ -177,7 +177,7 @@ def measured_peaks():
 
 
 def ncu_traffic():
-    p = REPO / "profiles" / "replace_tiles_c2_traffic.json"
+    p = REPO / "profiles" / "replace_super_c2_traffic.json"
     if p.exists():
         try:
             return json.loads(p.read_text())
