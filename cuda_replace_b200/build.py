@@ -17,7 +17,7 @@ REPO_DIR = PKG_DIR.parent
 CSRC = PKG_DIR / "csrc"
 LIB_NAME = "libcuda_replace.so"
 LIB_PATH = PKG_DIR / LIB_NAME
-SOURCES = ["replace_kernels.cu", "capi.cu", "noalloc.cu", "stream.cu"]
+SOURCES = ["replace_kernels.cu", "capi.cu", "noalloc.cu", "stream.cu", "batch.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -827,6 +827,97 @@ __global__ void __launch_bounds__(kThreads) query_tile_kernel(const __grid_const
   }
 }
 
+// ============================================================================ segmented plan
+// One CTA before every segmented launch: draw the launch's epoch (clearing the look-back
+// scratch when the 24-bit record tag or the 30-bit status epoch wraps), read every job's
+// input length, give each job its range of super-tiles and fill the super-tile -> job map.
+// A job whose result block holds an error or overflow epoch (an earlier launch of its chain
+// failed) or whose input is empty gets no super-tile and an empty output.
+__global__ void __launch_bounds__(1024) seg_plan_kernel(const __grid_constant__ SegLaunch sl) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_epoch, s_clear;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  if (tid == 0) {
+    uint32_t e = sl.epoch[1] + 1u;
+    uint32_t clear = 0;
+    if (e >= (1u << 30) - 2u) {
+      e = 1;
+      clear = 1;
+    } else if ((e & 0xFFFFFFu) == 0) {
+      e += 1;  // tag 0 is the cleared state
+      clear = 1;
+    }
+    s_epoch = e;
+    s_clear = clear;
+  }
+  __syncthreads();
+  if (s_clear) {
+    for (unsigned long long i = tid; i < sl.max_tiles; i += blockDim.x) {
+      sl.status[i] = 0;
+      sl.rec[2 * i] = 0;
+      sl.rec[2 * i + 1] = 0;
+    }
+  }
+  const uint32_t nj = *sl.njobs;
+  const unsigned long long S = (unsigned long long)sl.nsub * kTile;
+  uint32_t run = 0;  // super-tiles of the jobs before this chunk
+  for (uint32_t c0 = 0; c0 < nj; c0 += blockDim.x) {
+    const uint32_t j = c0 + tid;
+    uint32_t nt = 0;
+    if (j < nj) {
+      SegJob& J = sl.jobs[j];
+      const ApplyResult& r = sl.res[J.res];
+      const bool failed = r.error_epoch != 0u || r.overflow_epoch != 0u;
+      const unsigned long long n = failed ? 0ull : *J.n_dev;
+      const unsigned long long t = (n + S - 1ull) / S;
+      nt = t < 0xFFFFFFFFull ? (uint32_t)t : 0xFFFFFFFFu;
+      if (nt == 0) *J.len_out = 0;
+    }
+    // block exclusive scan of nt
+    uint32_t x = nt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= (uint32_t)d) x += o;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t y = lane < (blockDim.x >> 5) ? s_warp[lane] : 0u;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, y, d);
+        if (lane >= (uint32_t)d) y += o;
+      }
+      s_warp[lane] = y;
+    }
+    __syncthreads();
+    const uint32_t excl = (warp ? s_warp[warp - 1] : 0u) + x - nt;
+    const uint32_t chunk_total = s_warp[31];
+    if (j < nj) {
+      SegJob& J = sl.jobs[j];
+      const uint32_t base = run + excl;
+      J.tile_base = base;
+      J.ntiles = nt;
+      if ((unsigned long long)base + nt <= sl.max_tiles)
+        for (uint32_t i = 0; i < nt; ++i) sl.tile_job[base + i] = j;
+    }
+    run += chunk_total;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (run > sl.max_tiles) {
+      // more super-tiles than the scratch holds: run nothing, fail every job
+      *sl.total = 0;
+      for (uint32_t j = 0; j < nj; ++j) sl.res[sl.jobs[j].res].error_epoch = 0xFFFFFFFFu;
+    } else {
+      *sl.total = run;
+    }
+    sl.epoch[0] += 1u;
+    sl.epoch[1] = s_epoch;
+  }
+}
+
 // ============================================================================ held tail
 // Streaming: copy the last P bytes of buf[0, min(*total, cap)) to dst, where *total is the
 // length a previous launch left in device memory. Bytes before position 0 read as zero.
@@ -875,14 +966,16 @@ __host__ __device__ __forceinline__ uint32_t stage_ratio(uint32_t L, uint32_t R)
   return r < 3 ? r : 3;
 }
 
-__host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_t L, uint32_t R, uint32_t nsub) {
+// ratio: output staging per input byte (0: from L and R; a segmented launch passes the largest).
+__host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_t L, uint32_t R, uint32_t nsub,
+                                                          uint32_t ratio = 0) {
   LayoutS s{};
   uint32_t off = 0;
   s.inbytes = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16) + 32;
   s.in0 = off;
   off += kNBuf * s.inbytes;
   {
-    const uint32_t words = (2048u * stage_ratio(L, R) + 48u) / 4u;
+    const uint32_t words = (2048u * (ratio ? ratio : stage_ratio(L, R)) + 48u) / 4u;
     s.wstage_words = words + words / 32u + 2u;
   }
   s.outb = off;
@@ -1512,9 +1605,82 @@ struct LoadRing {
   __device__ __forceinline__ void shift() { iq = 0; iph = 0; ij = 0; }
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid_constant__ ReplaceParams p) {
+// Input length, output range and super-tile count of the job described by p.
+struct JobDims {
+  unsigned long long n_all, n, n16;
+  uint32_t NT, carry0, want_a;
+};
+__device__ __forceinline__ JobDims job_dims(const ReplaceParams& p, unsigned long long S) {
+  JobDims d;
+  // n_all bytes are in the buffer (matches may reach up to it); output covers the first n
+  d.n_all = p.n_dev ? min(*p.n_dev, p.n_cap ? p.n_cap : ~0ull) : p.n;
+  d.n = d.n_all > p.hold ? d.n_all - p.hold : 0ull;
+  d.n16 = (d.n_all + 15ull) & ~15ull;
+  d.NT = (uint32_t)min((d.n + S - 1ull) / S, (unsigned long long)p.num_tiles);
+  d.carry0 = p.carry0_dev ? *p.carry0_dev : p.carry0;
+  d.want_a = align_up_u32(kTile + (p.L > 1 ? p.L - 1 : 0), 16);
+  return d;
+}
+
+// Segmented launch, thread 0: claim the next super-tile of the launch; when it belongs to
+// another job than the one in sj, describe that job in sj. Returns the job-local super-tile
+// index, or 0xFFFFFFFF when the launch has no super-tile left.
+__device__ __forceinline__ uint32_t seg_claim(const SegLaunch& sl, ReplaceParams& sj, uint32_t* cur_job,
+                                              uint32_t* newjob) {
+  const uint32_t g = atomicAdd(sl.sched, 1u);
+  if (g >= *sl.total) return 0xFFFFFFFFu;
+  const uint32_t j = sl.tile_job[g];
+  const SegJob& J = sl.jobs[j];
+  const uint32_t base = J.tile_base;
+  if (j != *cur_job) {
+    *cur_job = j;
+    *newjob = 1u;
+    const SegPair& Q = sl.pairs[J.pair];
+    sj.in = J.in;
+    sj.out = J.out;
+    sj.n = *J.n_dev;
+    sj.out_cap = J.out_cap;
+    sj.block_before = 0;
+    sj.stride_mask = Q.stride_mask;
+    sj.L = Q.L;
+    sj.R = Q.R;
+    sj.mode = Q.mode;
+    sj.num_tiles = J.ntiles;
+    sj.epoch = sl.epoch[1];
+    sj.agg_entries = Q.agg_entries;
+    sj.p4 = Q.p4;
+    sj.m4 = Q.m4;
+    sj.inv_l = Q.inv_l;
+    sj.nsub = sl.nsub;
+    sj.status = sl.status + base;
+    sj.incl = sl.incl + base;
+    sj.agg = sl.agg + (unsigned long long)base * sl.agg_stride;
+    sj.res = sl.res + J.res;
+    sj.tile_last = sl.tile_last + base;
+    sj.rec = sl.rec + 2ull * base;
+    sj.n_dev = nullptr;
+    sj.len_out = J.len_out;
+    sj.carry0_dev = nullptr;
+    sj.carry_out = nullptr;
+    sj.hold = 0;
+    sj.n_cap = 0;
+    sj.len_bias = 0;
+    sj.carry0 = 0;
+    sj.pat_ext = Q.pat;
+    sj.rep_ext = Q.rep;
+  }
+  return g - base;
+}
+
+// One kernel for one apply (SEG = false: the job is the launch parameter pk) and for a
+// segmented launch over a job table (SEG = true: the job of each super-tile is looked up
+// and described in shared memory).
+template <int MODE, bool SEG>
+__global__ void __launch_bounds__(kThreads, 3)
+    replace_super_kernel(const __grid_constant__ ReplaceParams pk, const __grid_constant__ SegLaunch sl) {
   extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ ReplaceParams s_job;           // segmented launch: the job of the current super-tile
+  __shared__ uint32_t s_jobid, s_newjob;    // segmented launch: that job's index; its pattern is not staged yet
   __shared__ __align__(8) uint64_t s_bar[kNBuf];
   __shared__ uint32_t s_scan2[2][kWarps];  // alternating buffers of block_excl_scan1
   __shared__ uint32_t s_q[2];               // the super-tile this CTA works on
@@ -1526,45 +1692,54 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   __shared__ uint32_t s_wcnt[kMaxSub * kWarps];   // kModeFree: kept count per (sub-tile, warp)
   __shared__ uint32_t s_wcend[kMaxSub * kWarps];  // kModeFree: max cover end per (sub-tile, warp)
 
-  const uint32_t L = p.L, R = p.R, nsub = p.nsub;
-  const LayoutS lay = make_layout_s(MODE, L, R, nsub);
+  const ReplaceParams& p = SEG ? s_job : pk;
+  unsigned int* const sched = SEG ? sl.sched : &pk.res->tile_counter;  // claim counter, then finished CTAs
+  const uint32_t nsub = SEG ? sl.nsub : pk.nsub;
+  const LayoutS lay = SEG ? make_layout_s(MODE, sl.Lmax, sl.Rmax, nsub, 3u) : make_layout_s(MODE, pk.L, pk.R, nsub);
   uint8_t* ps = smem + lay.pat;
   uint8_t* rs = smem + lay.rep;
   uint8_t* ob = smem + lay.outb;
   uint64_t* masks = reinterpret_cast<uint64_t*>(smem + lay.masks);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t sb = tid * kSeg;
-  // n_all bytes are in the buffer (matches may reach up to it); output covers the first n
-  const unsigned long long n_all = p.n_dev ? min(*p.n_dev, p.n_cap ? p.n_cap : ~0ull) : p.n;
-  const unsigned long long n = n_all > p.hold ? n_all - p.hold : 0ull;
-  const unsigned long long n16 = (n_all + 15ull) & ~15ull;
   const unsigned long long S = (unsigned long long)nsub * kTile;
-  const uint32_t want_a = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16);
-  const uint32_t NT = (uint32_t)min((n + S - 1ull) / S, (unsigned long long)p.num_tiles);
-  const uint32_t carry0 = p.carry0_dev ? *p.carry0_dev : p.carry0;
-  if (NT == 0 && blockIdx.x == 0 && threadIdx.x == 0) {  // nothing to emit: still report
-    if (p.len_out) *p.len_out = p.len_bias;
-    if (p.carry_out) *p.carry_out = carry0 > n ? carry0 - (uint32_t)n : 0u;
-    p.res->out_len = 0;
-    p.res->kept = 0;
-  }
-  const bool warp_stage = R <= 3u * L;  // every warp's output fits its staging area
-
-  {
-    const uint8_t* psrc = L <= (uint32_t)kInlineMax ? p.pat : p.pat_ext;
-    const uint8_t* rsrc = R <= (uint32_t)kInlineMax ? p.rep : p.rep_ext;
+  // the job's dimensions and pattern: once (one apply) or whenever the job changes (segmented)
+  uint32_t L = 0, R = 0, NT = 0, carry0 = 0, want_a = 0, step4 = 0, step512 = 0;
+  unsigned long long n_all = 0, n = 0, n16 = 0;
+  bool warp_stage = false, rep_table = false;
+  auto setup_job = [&]() {
+    const JobDims d = job_dims(p, S);
+    n_all = d.n_all;
+    n = d.n;
+    n16 = d.n16;
+    NT = d.NT;
+    carry0 = d.carry0;
+    want_a = d.want_a;
+    L = p.L;
+    R = p.R;
+    warp_stage = R <= 3u * L;  // every warp's output fits its staging area
+    rep_table = R >= 1u && R <= 64u;
+    step4 = R ? 4u % R : 0u;
+    step512 = R ? 512u % R : 0u;
+    const uint8_t* psrc = (!SEG && L <= (uint32_t)kInlineMax) ? p.pat : p.pat_ext;
+    const uint8_t* rsrc = (!SEG && R <= (uint32_t)kInlineMax) ? p.rep : p.rep_ext;
     for (uint32_t i = tid; i < L; i += kThreads) ps[i] = psrc[i];
     // the replacement repeated: rs[i] = rep[i mod R] for i < R + 16
     for (uint32_t i = tid; i < R + 16; i += kThreads) rs[i] = R ? rsrc[i % R] : (uint8_t)0;
+    if (rep_table) {
+      uint8_t* t16 = smem + lay.tab16;
+      for (uint32_t i = tid; i < R * 16u; i += kThreads) t16[i] = rsrc[((i >> 4) + (i & 15u)) % R];
+    }
+  };
+  if (!SEG) {
+    setup_job();
+    if (NT == 0 && blockIdx.x == 0 && threadIdx.x == 0) {  // nothing to emit: still report
+      if (p.len_out) *p.len_out = p.len_bias;
+      if (p.carry_out) *p.carry_out = carry0 > n ? carry0 - (uint32_t)n : 0u;
+      p.res->out_len = 0;
+      p.res->kept = 0;
+    }
   }
-  const bool rep_table = R >= 1u && R <= 64u;
-  if (rep_table) {
-    const uint8_t* rsrc = R <= (uint32_t)kInlineMax ? p.rep : p.rep_ext;
-    uint8_t* t16 = smem + lay.tab16;
-    for (uint32_t i = tid; i < R * 16u; i += kThreads) t16[i] = rsrc[((i >> 4) + (i & 15u)) % R];
-  }
-  const uint32_t step4 = R ? 4u % R : 0u;
-  const uint32_t step512 = R ? 512u % R : 0u;
   uint32_t nscan = 0;  // block_excl_scan1 calls so far (selects the scratch buffer)
 
   // ---- load ring: thread 0 issues loads in the order they are consumed: for the current
@@ -1574,18 +1749,42 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
   if (tid == 0) {
     for (int b = 0; b < kNBuf; ++b) mbar_init(&s_bar[b], 1);
     fence_mbar_init();
-    const uint32_t first = atomicAdd(&p.res->tile_counter, 1u);
-    s_q[0] = first < NT ? first : NT;
+    if (SEG) {
+      s_jobid = 0xFFFFFFFFu;
+      s_newjob = 0;
+      s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
+    } else {
+      const uint32_t first = atomicAdd(sched, 1u);
+      s_q[0] = first < NT ? first : NT;
+    }
     s_q[1] = 0xFFFFFFFFu;
     s_fail = 0;
   }
   __syncthreads();
-  if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+  if (tid == 0) {
+    if (SEG) {
+      if (s_q[0] != 0xFFFFFFFFu) {
+        const JobDims d = job_dims(p, S);
+        ring.issue(p, smem, lay, s_bar, s_q, S, d.n16, d.want_a, d.n, d.NT);
+      }
+    } else {
+      ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+    }
+  }
 
   for (;;) {
     __syncthreads();
     const uint32_t t = s_q[0];
-    if (t >= NT) break;
+    if (SEG) {
+      if (t == 0xFFFFFFFFu) break;
+      if (s_newjob) {  // a super-tile of another job: its dimensions and pattern
+        setup_job();
+        __syncthreads();
+        if (tid == 0) s_newjob = 0;
+      }
+    } else if (t >= NT) {
+      break;
+    }
     const uint32_t m = subs_in_tile(t, S, n, nsub);
     const unsigned long long tstart = (unsigned long long)t * S;
 
@@ -2090,22 +2289,30 @@ __global__ void __launch_bounds__(kThreads, 3) replace_super_kernel(const __grid
     // claim the next super-tile only now, when its pass A starts: a super-tile claimed
     // early but started late would hold up the look-back of every later super-tile
     if (tid == 0) {
-      const uint32_t nx = atomicAdd(&p.res->tile_counter, 1u);
-      s_q[0] = nx < NT ? nx : NT;
       s_q[1] = 0xFFFFFFFFu;
       ring.shift();
       s_fail = 0;
-      ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+      if (SEG) {
+        s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
+        if (s_q[0] != 0xFFFFFFFFu) {
+          const JobDims d = job_dims(p, S);
+          ring.issue(p, smem, lay, s_bar, s_q, S, d.n16, d.want_a, d.n, d.NT);
+        }
+      } else {
+        const uint32_t nx = atomicAdd(sched, 1u);
+        s_q[0] = nx < NT ? nx : NT;
+        ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+      }
     }
   }
 
   if (tid == 0) {
     bulk_wait_all();
     __threadfence();
-    const unsigned int d = atomicAdd(&p.res->done_ctas, 1u);
+    const unsigned int d = atomicAdd(sched + 1, 1u);
     if (d == gridDim.x - 1) {
-      atomicExch(&p.res->tile_counter, 0u);
-      atomicExch(&p.res->done_ctas, 0u);
+      atomicExch(sched, 0u);
+      atomicExch(sched + 1, 0u);
       __threadfence();
     }
   }
@@ -2344,7 +2551,7 @@ cudaError_t launch_super_mode(const ReplaceParams& p, cudaStream_t st, int* grid
   {
     std::lock_guard<std::mutex> g(mu);
     if (!(attr_dev_mask & (1ull << (dev & 63)))) {
-      cudaError_t e = cudaFuncSetAttribute(replace_super_kernel<MODE>,
+      cudaError_t e = cudaFuncSetAttribute(replace_super_kernel<MODE, false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
       if (e != cudaSuccess) return e;
       e = cudaFuncSetAttribute(query_super_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2354,14 +2561,14 @@ cudaError_t launch_super_mode(const ReplaceParams& p, cudaStream_t st, int* grid
     }
   }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, replace_super_kernel<MODE>, kThreads,
-                                                                smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, replace_super_kernel<MODE, false>,
+                                                                kThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   long long grid = (long long)per_sm * device_sm_count();
   if (grid > (long long)p.num_tiles) grid = p.num_tiles;
   if (grid < 1) grid = 1;
-  replace_super_kernel<MODE><<<(unsigned)grid, kThreads, smem, st>>>(p);
+  replace_super_kernel<MODE, false><<<(unsigned)grid, kThreads, smem, st>>>(p, SegLaunch{});
   if (grid_out) *grid_out = (int)grid;
   return cudaGetLastError();
 }
@@ -2405,6 +2612,80 @@ cudaError_t launch_move_tail(const uint8_t* buf, const unsigned long long* total
                              uint32_t P, uint8_t* dst, cudaStream_t st) {
   move_tail_kernel<<<1, 256, 0, st>>>(buf, total, cap, P, dst);
   return cudaGetLastError();
+}
+
+uint32_t seg_smem_bytes(const SegLaunch& sl) { return make_layout_s(sl.mode, sl.Lmax, sl.Rmax, sl.nsub, 3u).total; }
+
+namespace {
+template <int MODE>
+int seg_occupancy(uint32_t smem) {
+  static std::mutex mu;
+  static unsigned long long attr_dev_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!(attr_dev_mask & (1ull << (dev & 63)))) {
+      if (cudaFuncSetAttribute(replace_super_kernel<MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               220 * 1024) != cudaSuccess)
+        return -1;
+      attr_dev_mask |= 1ull << (dev & 63);
+    }
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, replace_super_kernel<MODE, true>, kThreads, smem) !=
+      cudaSuccess)
+    return -1;
+  return per_sm < 1 ? 1 : per_sm;
+}
+}  // namespace
+
+int seg_ctas_per_sm(const SegLaunch& sl) {
+  const uint32_t smem = seg_smem_bytes(sl);
+  return sl.mode == kModeFree ? seg_occupancy<kModeFree>(smem) : seg_occupancy<kModeSmall>(smem);
+}
+
+cudaError_t launch_seg(const SegLaunch& sl, cudaStream_t st, int grid_ctas) {
+  if (sl.mode != kModeFree && sl.mode != kModeSmall) return cudaErrorInvalidValue;
+  if (sl.Lmax > kSegMaxL || sl.Rmax > kSegMaxR || sl.nsub < 1 || sl.nsub > (uint32_t)kMaxSub)
+    return cudaErrorInvalidValue;
+  if (sl.mode == kModeSmall && sl.nsub * sl.Lmax > 128u) return cudaErrorInvalidValue;
+  const uint32_t smem = seg_smem_bytes(sl);
+  int grid = grid_ctas;
+  if (grid <= 0) {  // (a caller that passes the grid has called seg_ctas_per_sm for this mode before)
+    const int per_sm = seg_ctas_per_sm(sl);
+    if (per_sm < 0) return cudaErrorUnknown;
+    grid = per_sm * device_sm_count();
+  }
+  seg_plan_kernel<<<1, 1024, 0, st>>>(sl);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (sl.mode == kModeFree)
+    replace_super_kernel<kModeFree, true><<<(unsigned)grid, kThreads, smem, st>>>(ReplaceParams{}, sl);
+  else
+    replace_super_kernel<kModeSmall, true><<<(unsigned)grid, kThreads, smem, st>>>(ReplaceParams{}, sl);
+  return cudaGetLastError();
+}
+
+bool make_seg_pair(SegPair& q, const uint8_t* pat, uint32_t L, const uint8_t* rep, uint32_t R) {
+  if (L < 1 || L > kSegMaxL || R > kSegMaxR) return false;
+  ReplaceParams p;
+  memset(&p, 0, sizeof(p));
+  prepare_pattern_fields(p, pat, L);
+  if (p.mode != kModeFree && p.mode != kModeSmall) return false;
+  if (p.mode == kModeSmall && super_nsub(p.mode, L) == 0) return false;
+  memset(&q, 0, sizeof(q));
+  q.stride_mask = p.stride_mask;
+  q.L = L;
+  q.R = R;
+  q.mode = p.mode;
+  q.p4 = p.p4;
+  q.m4 = p.m4;
+  q.inv_l = p.inv_l;
+  q.agg_entries = p.agg_entries;
+  memcpy(q.pat, pat, L);
+  if (R) memcpy(q.rep, rep, R);
+  return true;
 }
 
 cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const uint8_t* rep_dev, uint32_t R,

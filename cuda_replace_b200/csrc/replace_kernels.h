@@ -104,6 +104,56 @@ struct ReplaceParams {
   uint8_t rep[kInlineMax];
 };
 
+// ---- Segmented launch: many jobs in ONE launch of the super-tile kernel. Each job has its
+// own input, output and (pattern, replacement); work is split by super-tiles across all jobs,
+// not by jobs: super-tile g of the launch belongs to job tile_job[g], at local index
+// g - jobs[tile_job[g]].tile_base. A plan kernel (one CTA) reads every job's input length
+// from device memory, numbers the super-tiles and draws a fresh epoch, so a sequence of
+// segmented launches chains on the device and can be replayed from a CUDA graph.
+constexpr uint32_t kSegMaxL = 32;  // longest pattern of a segmented launch
+constexpr uint32_t kSegMaxR = 64;  // longest replacement of a segmented launch
+
+struct SegPair {                   // one (pattern, replacement) and its derived fields
+  unsigned long long stride_mask;
+  unsigned int L, R, mode, p4, m4, inv_l, agg_entries, pad;
+  uint8_t pat[kSegMaxL];
+  uint8_t rep[kSegMaxR];
+};
+
+struct SegJob {                    // one job of a segmented launch
+  const uint8_t* in;               // 16-byte aligned, readable up to its length rounded up to 16
+  uint8_t* out;                    // 16-byte aligned
+  const unsigned long long* n_dev; // input length (device)
+  unsigned long long* len_out;     // receives the output length (device)
+  unsigned long long out_cap;
+  unsigned int pair;               // index into SegLaunch::pairs
+  unsigned int res;                // index of the job's result block
+  unsigned int tile_base;          // written by the plan kernel
+  unsigned int ntiles;             // written by the plan kernel
+  unsigned int pad[2];
+};
+
+struct SegLaunch {
+  SegJob* jobs;
+  const unsigned int* njobs;       // device: jobs in this launch
+  const SegPair* pairs;
+  ApplyResult* res;                // per job; a nonzero error or overflow epoch marks the job failed
+  unsigned int* total;             // device: super-tiles of this launch (plan kernel)
+  unsigned int* tile_job;          // [max_tiles]: super-tile -> job (plan kernel)
+  unsigned int* sched;             // [2]: claim counter, finished CTAs (reset by the last CTA)
+  unsigned int* epoch;             // [2]: launch counter (plan kernel) and the current epoch
+  uint32_t* status;                // look-back scratch shared by the launches of one stream
+  TileIncl* incl;
+  unsigned long long* agg;
+  long long* tile_last;
+  unsigned long long* rec;
+  unsigned int max_tiles;          // capacity of the scratch arrays, in super-tiles
+  unsigned int agg_stride;         // agg entries per super-tile (the largest L of the launch)
+  unsigned int mode;               // CarryMode of every pair in the launch
+  unsigned int Lmax, Rmax;         // largest pattern and replacement (shared-memory layout)
+  unsigned int nsub;               // 16 KiB sub-tiles per super-tile
+};
+
 // Host helpers (replace_kernels.cu).
 // Fills the pattern-derived fields of p (mode, p4, m4, inv_l, stride_mask, agg_entries).
 void prepare_pattern_fields(ReplaceParams& p, const uint8_t* pat, uint32_t L);
@@ -123,6 +173,17 @@ cudaError_t launch_query(const ReplaceParams& p, cudaStream_t st);
 // Copy the last P bytes of buf[0, min(*total, cap)) to dst (streaming: a stage's held tail).
 cudaError_t launch_move_tail(const uint8_t* buf, const unsigned long long* total, unsigned long long cap,
                              uint32_t P, uint8_t* dst, cudaStream_t st);
+// Segmented launch (sl.mode free or small): the plan kernel, then the super-tile kernel over
+// every job's super-tiles. grid_ctas = 0 picks the occupancy-limited persistent grid; a
+// caller passing its own grid must have called seg_ctas_per_sm for the mode once (it sets the
+// kernel's shared-memory limit), after which launch_seg makes no other runtime call than the
+// two launches (so it can be captured in a CUDA graph).
+cudaError_t launch_seg(const SegLaunch& sl, cudaStream_t st, int grid_ctas);
+// Dynamic shared memory of a segmented launch, and its CTAs per SM.
+uint32_t seg_smem_bytes(const SegLaunch& sl);
+int seg_ctas_per_sm(const SegLaunch& sl);
+// Fills a SegPair from (pat, L, rep, R); false when the pair does not fit a segmented launch.
+bool make_seg_pair(SegPair& q, const uint8_t* pat, uint32_t L, const uint8_t* rep, uint32_t R);
 // bytes.replace with an empty pattern: rep before every byte and at the end.
 cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const uint8_t* rep_dev,
                                  uint32_t R, uint8_t* out, cudaStream_t st);

@@ -49,6 +49,21 @@ def _bind(lib: C.CDLL, name: str, argtypes, restype, optional: bool = False) -> 
     fn.restype = restype
 
 
+class ServerStats(C.Structure):
+    """CudaReplaceServerStats (include/cuda_replace.h)."""
+    _fields_ = [("jobs_done", C.c_ulonglong), ("jobs_via_session", C.c_ulonglong), ("batches", C.c_ulonglong),
+                ("bytes_in", C.c_ulonglong), ("bytes_out", C.c_ulonglong), ("kernel_launches", C.c_ulonglong),
+                ("graph_launches", C.c_ulonglong), ("pending", C.c_ulonglong), ("arena_bytes", C.c_ulonglong),
+                ("arena_peak_bytes", C.c_ulonglong), ("p50_us", C.c_double), ("p99_us", C.c_double),
+                ("max_us", C.c_double), ("tile_bytes", C.c_uint * 3), ("grid_ctas", C.c_int * 3)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["tile_bytes"] = list(self.tile_bytes)
+        d["grid_ctas"] = list(self.grid_ctas)
+        return d
+
+
 class CudaReplaceLib:
     """Loads libcuda_replace.so and binds its C ABI (reference: py:36-141)."""
 
@@ -89,6 +104,18 @@ class CudaReplaceLib:
               C.c_int, optional=True)
         _bind(lib, "cuda_replace_device_result", [c_void_p, c_size_t_p, C.POINTER(C.c_ulonglong)], C.c_int,
               optional=True)
+        _bind(lib, "cuda_replace_server_open", [C.POINTER(c_void_p), c_size_t, C.c_int], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_submit",
+              [c_void_p, c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int,
+               C.POINTER(C.c_ulonglong)], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_wait",
+              [c_void_p, C.c_ulonglong, C.c_int, C.POINTER(c_uint8_p), c_size_t_p], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_stats", [c_void_p, C.POINTER(ServerStats)], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_reset_stats", [c_void_p], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_close", [c_void_p], None, optional=True)
+        _bind(lib, "cuda_replace_jobs",
+              [C.c_int, c_uint8_pp, c_size_t_p, c_int_p, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p,
+               c_uint8_pp, c_size_t_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_stream",
               [c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t,
                C.POINTER(c_uint8_p), c_size_t_p], C.c_int, optional=True)
@@ -249,6 +276,119 @@ class Session:
         if self.h:
             self.lib.lib.cuda_replace_close(self.h)
             self.h = c_void_p(None)
+
+
+class Server:
+    """Request loop over batched segmented launches (no counterpart in the reference).
+
+    ``submit(data, pairs)`` queues a job (its input and its own sequence of pairs) and returns
+    a ticket; ``wait(ticket)`` returns the job's result, equal to the chained bytes.replace.
+    Jobs that arrive while a batch is on the GPU are admitted to the next batch as device
+    memory (``hbm_budget`` bytes, 0 = 40% of the free memory) and one of two batch slots free
+    up; ``stats()`` reports throughput and p50/p99 latency from submit to result."""
+
+    def __init__(self, lib: CudaReplaceLib, hbm_budget: int = 0, max_jobs_per_batch: int = 0):
+        if getattr(lib.lib, "cuda_replace_server_open", None) is None:
+            raise RuntimeError("this libcuda_replace.so has no server entry points")
+        self.lib = lib
+        self.h = c_void_p()
+        rc = lib.lib.cuda_replace_server_open(C.byref(self.h), c_size_t(int(hbm_budget)), C.c_int(max_jobs_per_batch))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_server_open failed rc={rc}")
+
+    def __enter__(self) -> "Server":
+        return self
+
+    def __exit__(self, exc_type, exc, tb):
+        self.close()
+
+    def submit(self, data, pairs: Sequence[Tuple[bytes, bytes]]) -> int:
+        keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(pairs)
+        mv = memoryview(data)
+        n = mv.nbytes
+        if not n:
+            holder, src_ptr = None, c_uint8_p()
+        elif isinstance(data, bytes) or mv.readonly:
+            holder = data if isinstance(data, bytes) else bytes(mv)
+            src_ptr = C.cast(C.c_char_p(holder), c_uint8_p)
+        else:
+            holder = (C.c_uint8 * n).from_buffer(mv)
+            src_ptr = C.cast(holder, c_uint8_p)
+        ticket = C.c_ulonglong(0)
+        rc = self.lib.lib.cuda_replace_server_submit(
+            self.h, src_ptr, c_size_t(n), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
+            C.cast(rep_ptrs, c_uint8_pp), C.cast(rep_lens, c_int_p), C.c_int(len(pairs)), C.byref(ticket))
+        del keep, holder
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_server_submit failed rc={rc}")
+        return int(ticket.value)
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> Optional[bytes]:
+        """The job's result; None when it is not done within timeout_ms (negative: no limit)."""
+        out_ptr = c_uint8_p()
+        out_len = c_size_t()
+        rc = self.lib.lib.cuda_replace_server_wait(self.h, C.c_ulonglong(ticket), C.c_int(timeout_ms),
+                                                   C.byref(out_ptr), C.byref(out_len))
+        if rc == 1:
+            return None
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_server_wait failed rc={rc}")
+        try:
+            return _bytes_at(out_ptr, out_len.value)
+        finally:
+            self.lib.lib.cuda_free_host(out_ptr)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        rc = self.lib.lib.cuda_replace_server_stats(self.h, C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_server_stats failed rc={rc}")
+        return st.as_dict()
+
+    def reset_stats(self) -> None:
+        self.lib.lib.cuda_replace_server_reset_stats(self.h)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.lib.cuda_replace_server_close(self.h)
+            self.h = c_void_p(None)
+
+
+def replace_jobs(lib: CudaReplaceLib, jobs: Sequence[Tuple[bytes, Sequence[Tuple[bytes, bytes]]]]) -> List[bytes]:
+    """Many independent jobs (input, pairs) in one call: each result equals the chained
+    bytes.replace of its job. Runs as batched segmented launches (cuda_replace_jobs)."""
+    fn = getattr(lib.lib, "cuda_replace_jobs", None)
+    if fn is None:
+        raise RuntimeError("this libcuda_replace.so has no cuda_replace_jobs")
+    nj = len(jobs)
+    if nj == 0:
+        return []
+    srcs = (c_uint8_p * nj)()
+    lens = (c_size_t * nj)()
+    counts = (C.c_int * nj)()
+    flat: List[Tuple[bytes, bytes]] = []
+    holders = []
+    for i, (data, pairs) in enumerate(jobs):
+        b = data if isinstance(data, bytes) else bytes(data)
+        holders.append(b)
+        srcs[i] = C.cast(C.c_char_p(b), c_uint8_p) if b else c_uint8_p()
+        lens[i] = len(b)
+        counts[i] = len(pairs)
+        flat.extend(pairs)
+    keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(flat)
+    outs = (c_uint8_p * nj)()
+    out_lens = (c_size_t * nj)()
+    rc = fn(C.c_int(nj), C.cast(srcs, c_uint8_pp), C.cast(lens, c_size_t_p), C.cast(counts, c_int_p),
+            C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p), C.cast(rep_ptrs, c_uint8_pp),
+            C.cast(rep_lens, c_int_p), C.cast(outs, c_uint8_pp), C.cast(out_lens, c_size_t_p))
+    del keep, holders
+    if rc != 0:
+        raise RuntimeError(f"cuda_replace_jobs failed rc={rc}")
+    res = []
+    for i in range(nj):
+        res.append(_bytes_at(outs[i], out_lens[i]))
+        lib.lib.cuda_free_host(outs[i])
+    return res
 
 
 def replace_unified(lib: CudaReplaceLib, src: bytes, pat: bytes, rep: bytes) -> bytes:

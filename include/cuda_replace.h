@@ -182,6 +182,63 @@ int cuda_replace_stream(const uint8_t* src, size_t n, const uint8_t** pats, cons
                         const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
                         uint8_t** out_host, size_t* out_len);
 
+/* ---- Batched jobs and serving. No counterpart in the reference, whose only batch is the
+ * sequential pair chain of one buffer (cuda_replace_apply_batch, cu:2465); a caller with many
+ * independent buffers there makes one unified() call per buffer and pair
+ * (cuda_replace_wrapper.py:124-141). Here many jobs (each an input and its own sequence of
+ * pairs) run together: round r applies every job's r-th pair in one segmented launch per
+ * carry class, work split by 16 KiB super-tiles across all jobs, with the rounds replayed from
+ * a CUDA graph and lengths passed between rounds on the device. Results equal, per job, the
+ * chained bytes.replace. Pairs outside the segmented limits (pattern 1-32 B, replacement up
+ * to 64 B, at most 16 pairs per job), and jobs whose output outgrows the buffers planned for
+ * them, run through a Session instead; the result is the same. */
+
+/* A server keeps its device memory (an arena of hbm_budget bytes; 0 = 40% of the free
+ * memory) for its lifetime. submit() copies the input and pairs, so the caller's buffers may
+ * be released when it returns. A dispatcher thread forms a batch whenever one of two batch
+ * slots is free, admitting queued requests in arrival order while their device footprint
+ * (input + two ping-pong buffers of up to 4x input + 1 MiB) fits the arena; requests that
+ * arrive while a batch runs form the next one, which runs beside it. max_jobs_per_batch: 0 =
+ * 4096. All calls are thread-safe. */
+typedef struct CudaReplaceServerStats {
+  unsigned long long jobs_done;         /* since open or the last reset_stats */
+  unsigned long long jobs_via_session;  /* of those, run through a Session */
+  unsigned long long batches;
+  unsigned long long bytes_in, bytes_out;
+  unsigned long long kernel_launches;   /* plan + segmented kernels enqueued (in graphs) */
+  unsigned long long graph_launches;
+  unsigned long long pending;           /* requests queued, not yet on the device */
+  unsigned long long arena_bytes, arena_peak_bytes;
+  double p50_us, p99_us, max_us;        /* latency: submit() to result ready */
+  unsigned int tile_bytes[3];           /* autotuned super-tile bytes: free, bordered L<=4, bordered L<=32 */
+  int grid_ctas[3];
+} CudaReplaceServerStats;
+
+int cuda_replace_server_open(void** srv, size_t hbm_budget, int max_jobs_per_batch);
+/* -1 NULL arguments or a negative length, -4 a pattern or replacement longer than
+ * CUDA_REPLACE_MAX_PATTERN, >0 a cudaError_t. *ticket identifies the request. */
+int cuda_replace_server_submit(void* srv, const uint8_t* src, size_t n,
+                               const uint8_t** pats, const int* pat_lens,
+                               const uint8_t** reps, const int* rep_lens, int count,
+                               unsigned long long* ticket);
+/* 0: done; *out_host (page-locked, release with cuda_free_host; NULL when empty) and
+ * *out_len receive the result and the ticket is retired. 1: not done within timeout_ms
+ * (negative: wait without limit). -1: unknown ticket. Other: the request's error code. */
+int cuda_replace_server_wait(void* srv, unsigned long long ticket, int timeout_ms,
+                             uint8_t** out_host, size_t* out_len);
+int cuda_replace_server_stats(void* srv, CudaReplaceServerStats* stats);
+int cuda_replace_server_reset_stats(void* srv);
+/* Finishes every submitted request, then releases the server. */
+void cuda_replace_server_close(void* srv);
+
+/* One call for many jobs: job i is srcs[i][0, src_lens[i]) with pair_counts[i] pairs, the
+ * pairs of all jobs concatenated in pats/pat_lens/reps/rep_lens. out_hosts[i] / out_lens[i]
+ * receive job i's result (release each with cuda_free_host). Runs on a server opened for the
+ * call. On an error no result is returned. */
+int cuda_replace_jobs(int njobs, const uint8_t** srcs, const size_t* src_lens, const int* pair_counts,
+                      const uint8_t** pats, const int* pat_lens, const uint8_t** reps, const int* rep_lens,
+                      uint8_t** out_hosts, size_t* out_lens);
+
 #ifdef __cplusplus
 }
 #endif
