@@ -310,18 +310,38 @@ class Engine {
   Slot slots[kSlots];
   Tuning tune;
   int max_jobs = 0;
+  crb::HostArena* hstage = nullptr;  // page-locked staging of inputs and results
+
+  // page-locked host memory: the staging area first, the pool when it is full
+  uint8_t* host_get(size_t n, cudaError_t* e) {
+    *e = cudaSuccess;
+    uint8_t* p = hstage ? hstage->alloc(n) : nullptr;
+    return p ? p : static_cast<uint8_t*>(crb::host_pinned_pool().get(n, e));
+  }
   std::atomic<unsigned long long> seg_launches{0}, graph_launches{0};
 
   cudaError_t init(size_t budget, int mj) {
     cudaGetDevice(&device);
     max_jobs = mj;
     cudaError_t e = arena.init(budget);
+    if (e == cudaSuccess) {
+      hstage = new crb::HostArena();
+      e = hstage->init(std::min<size_t>(4ull << 30, std::max<size_t>(64u << 20, budget / 4)));
+      if (e != cudaSuccess) {
+        delete hstage;
+        hstage = nullptr;
+      } else {
+        crb::host_arena_register(hstage);
+      }
+    }
     for (int i = 0; i < kSlots && e == cudaSuccess; ++i) e = slots[i].init(max_jobs);
     if (e == cudaSuccess) e = autotune();
     return e;
   }
   void destroy() {
     for (auto& s : slots) s.destroy();
+    if (hstage) crb::host_arena_close(hstage);  // freed once the callers release its last block
+    hstage = nullptr;
   }
 
   // Device footprint of a job: input + two ping-pong buffers (each + 64 B of read slack).
@@ -459,7 +479,6 @@ class Engine {
   cudaError_t finish(Slot& s, std::vector<Job*>* rerun) {
     cudaError_t e = cudaEventSynchronize(s.ev_meta);
     if (e != cudaSuccess) return e;
-    crb::PinnedPool& pool = crb::host_pinned_pool();
     uint8_t* base = arena.base();
     const int nj = (int)s.jobs.size();
     for (int i = 0; i < nj && e == cudaSuccess; ++i) {
@@ -474,7 +493,7 @@ class Engine {
       const size_t off = k == 0 ? j.off_in : ((k & 1) ? j.off_a : j.off_b);
       j.out_len = len;
       if (len) {
-        j.hout = static_cast<uint8_t*>(pool.get(len, &e));
+        j.hout = host_get(len, &e);
         if (!j.hout) break;
         e = cudaMemcpyAsync(j.hout, base + off, len, cudaMemcpyDeviceToHost, s.st);
       }
@@ -652,13 +671,12 @@ class Server {
     if (completer_.joinable()) completer_.join();
     if (fallback_.joinable()) fallback_.join();
     cudaSetDevice(device_);
-    eng_.destroy();
-    crb::PinnedPool& pool = crb::host_pinned_pool();
     for (auto& kv : jobs_) {
-      if (kv.second->hin) pool.put(kv.second->hin);
-      if (kv.second->hout) pool.put(kv.second->hout);
+      crb::host_free(kv.second->hin);
+      crb::host_free(kv.second->hout);
     }
     jobs_.clear();
+    eng_.destroy();
   }
 
   int submit(const uint8_t* src, size_t n, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
@@ -680,9 +698,9 @@ class Server {
     }
     if (!j->seg_ok) j->seg.clear();
     cudaError_t e;
-    j->hin = static_cast<uint8_t*>(crb::host_pinned_pool().get(n ? n : 1, &e));
+    j->hin = eng_.host_get(n ? n : 1, &e);
     if (!j->hin) return (int)e;
-    if (n) memcpy(j->hin, src, n);
+    if (n) crb::parallel_memcpy(j->hin, src, n);
     if (j->seg_ok) j->cap = job_capacity(*j);
     std::lock_guard<std::mutex> g(mu_);
     j->ticket = ++next_ticket_;
@@ -761,7 +779,7 @@ class Server {
     if (j->via_session) ++jobs_session_;
     bytes_in_ += j->n;
     bytes_out_ += j->out_len;
-    crb::host_pinned_pool().put(j->hin);
+    crb::host_free(j->hin);
     j->hin = nullptr;
     cv_.notify_all();
   }
@@ -870,7 +888,7 @@ class Server {
       running_fallback_ = true;
       lk.unlock();
       if (j->hout) {
-        crb::host_pinned_pool().put(j->hout);
+        crb::host_free(j->hout);
         j->hout = nullptr;
       }
       const int rc = run_with_session(*j);

@@ -35,6 +35,47 @@ PinnedPool& host_pinned_pool() {
   static PinnedPool* pool = new PinnedPool();  // never destroyed: CUDA may be torn down first at exit
   return *pool;
 }
+
+namespace {
+std::mutex g_arena_mu;
+std::vector<HostArena*>& arenas() {
+  static auto* v = new std::vector<HostArena*>();  // never destroyed, like the pool
+  return *v;
+}
+}  // namespace
+
+void host_arena_register(HostArena* a) {
+  std::lock_guard<std::mutex> g(g_arena_mu);
+  arenas().push_back(a);
+}
+
+void host_arena_close(HostArena* a) {
+  std::lock_guard<std::mutex> g(g_arena_mu);
+  if (a->close()) {
+    auto& v = arenas();
+    v.erase(std::remove(v.begin(), v.end(), a), v.end());
+    delete a;
+  }
+}
+
+void host_free(void* p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> g(g_arena_mu);
+    auto& v = arenas();
+    for (auto it = v.begin(); it != v.end(); ++it) {
+      if ((*it)->contains(p)) {
+        HostArena* a = *it;
+        if (a->release(p)) {  // closed and empty: the last block of a closed server's area
+          v.erase(it);
+          delete a;
+        }
+        return;
+      }
+    }
+  }
+  host_pinned_pool().put(p);
+}
 }  // namespace crb
 
 #define CR_EXPORT extern "C" __attribute__((visibility("default")))
@@ -628,7 +669,7 @@ void cache_give(Session* s) {
 CR_EXPORT const char* cuda_replace_version(void) { return "cuda_replace_b200 1.0 sm_100a single-pass look-back"; }
 
 CR_EXPORT void cuda_free_host(void* p) {
-  if (p) pinned_pool().put(p);
+  if (p) crb::host_free(p);
 }
 
 CR_EXPORT int cuda_replace_open(void** ph, const uint8_t* src, size_t len) {

@@ -5,9 +5,11 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <iterator>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -73,5 +75,110 @@ class PinnedPool {
 
 // The process-wide pool (never destroyed: CUDA may be torn down first at exit).
 PinnedPool& host_pinned_pool();
+
+// memcpy split over up to 8 host threads when it is large (pageable <-> page-locked staging).
+inline void parallel_memcpy(void* dst, const void* src, size_t n) {
+  const size_t kMin = 8u << 20;
+  const unsigned hw = std::thread::hardware_concurrency();
+  const unsigned t = hw ? (hw < 8u ? hw : 8u) : 4u;
+  if (n < kMin || t < 2) {
+    memcpy(dst, src, n);
+    return;
+  }
+  const size_t part = pool_round_up((n + t - 1) / t, 4096);
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < t; ++i) {
+    const size_t a = part * i;
+    if (a >= n) break;
+    const size_t len = part < n - a ? part : n - a;
+    th.emplace_back([=]() { memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, len); });
+  }
+  memcpy(dst, src, part < n ? part : n);
+  for (auto& x : th) x.join();
+}
+
+// First-fit sub-allocator over one page-locked block: a server's host staging area, pinned
+// once instead of per request. Blocks handed to callers are released with cuda_free_host
+// (host_free below finds the owning area); an area closed by its server is freed when its
+// last block comes back.
+class HostArena {
+ public:
+  ~HostArena() {
+    if (base_) cudaFreeHost(base_);
+  }
+  cudaError_t init(size_t bytes) {
+    bytes = pool_round_up(bytes ? bytes : 1, 2u << 20);
+    cudaError_t e = cudaMallocHost(&base_, bytes);
+    if (e != cudaSuccess) {
+      base_ = nullptr;
+      return e;
+    }
+    size_ = bytes;
+    free_[0] = bytes;
+    return cudaSuccess;
+  }
+  uint8_t* alloc(size_t n) {
+    n = pool_round_up(n ? n : 1, 256);
+    std::lock_guard<std::mutex> g(mu_);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= n) {
+        const size_t off = it->first, rest = it->second - n;
+        free_.erase(it);
+        if (rest) free_[off + n] = rest;
+        used_[off] = n;
+        return base_ + off;
+      }
+    }
+    return nullptr;
+  }
+  bool contains(const void* p) const {
+    const uint8_t* q = static_cast<const uint8_t*>(p);
+    return base_ && q >= base_ && q < base_ + size_;
+  }
+  // returns true when the area is closed and now empty
+  bool release(const void* p) {
+    std::lock_guard<std::mutex> g(mu_);
+    size_t start = (size_t)(static_cast<const uint8_t*>(p) - base_);
+    auto u = used_.find(start);
+    if (u == used_.end()) return false;
+    size_t len = u->second;
+    used_.erase(u);
+    auto nx = free_.lower_bound(start);
+    if (nx != free_.end() && start + len == nx->first) {
+      len += nx->second;
+      nx = free_.erase(nx);
+    }
+    if (nx != free_.begin()) {
+      auto pv = std::prev(nx);
+      if (pv->first + pv->second == start) {
+        start = pv->first;
+        len += pv->second;
+        free_.erase(pv);
+      }
+    }
+    free_[start] = len;
+    return closed_ && used_.empty();
+  }
+  // the owner is gone; true when nothing is outstanding (the area can be freed now)
+  bool close() {
+    std::lock_guard<std::mutex> g(mu_);
+    closed_ = true;
+    return used_.empty();
+  }
+
+ private:
+  std::mutex mu_;
+  uint8_t* base_ = nullptr;
+  size_t size_ = 0;
+  bool closed_ = false;
+  std::map<size_t, size_t> free_, used_;
+};
+
+// Registry of the live host areas (defined in capi.cu).
+void host_arena_register(HostArena* a);
+// The owner closes its area: freed now, or when its last block is released.
+void host_arena_close(HostArena* a);
+// Release a block handed to a caller: into its host area, else into the pool.
+void host_free(void* p);
 
 }  // namespace crb

@@ -44,26 +44,7 @@ constexpr int kUnsupported = -7;  // a pair outside the limits of this path
 
 size_t rup(size_t x, size_t q) { return (x + q - 1) / q * q; }
 
-// memcpy split over a few host threads (pageable source into page-locked staging)
-void parallel_memcpy(void* dst, const void* src, size_t n) {
-  const size_t kMin = 8u << 20;
-  const unsigned hw = std::thread::hardware_concurrency();
-  const unsigned t = hw ? std::min(8u, hw) : 4u;
-  if (n < kMin || t < 2) {
-    memcpy(dst, src, n);
-    return;
-  }
-  const size_t part = rup((n + t - 1) / t, 4096);
-  std::vector<std::thread> th;
-  for (unsigned i = 1; i < t; ++i) {
-    const size_t a = part * i;
-    if (a >= n) break;
-    const size_t len = std::min(part, n - a);
-    th.emplace_back([=]() { memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, len); });
-  }
-  memcpy(dst, src, std::min(part, n));
-  for (auto& x : th) x.join();
-}
+using crb::parallel_memcpy;
 
 bool is_pinned(const void* p) {
   cudaPointerAttributes a;
