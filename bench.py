@@ -11,6 +11,9 @@ value:  device-resident inputs (HBM), K steps timed with CUDA events on the laun
 e2e:    the same step through the reference-facing C ABI call cuda_replace_unified with
         page-locked host inputs: H2D, kernel, D2H of the result inside the timed region.
 cpu_baseline: CPython bytes.replace (single thread) on a bounded sample of the same cases.
+batched: a sample of the 10,000-job workload through the request loop (segmented launches,
+        CUDA graphs, HBM-budget admission): jobs/s closed loop and p50/p99 under Poisson
+        arrivals, against the same jobs as per-job plain unified() calls (--no-batched skips).
 --impl reference: the reference's CPU path (bytes.replace) alone, on all three cases.
 
 Multi-GPU: the path does not shard across GPUs here (replicas only): under torchrun each
@@ -50,6 +53,12 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cases", default="0,1,2", help="comma-separated subset of the three cases (profiling)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched/served jobs sample")
+    ap.add_argument("--workload", choices=["single", "chain", "stream"], default="single",
+                    help="single: the single-pair workload (default line); chain: 4 GiB text x 128 pairs "
+                         "through apply_batch; stream: 16 GiB text x 8 pairs through gpu_replace_streaming")
+    ap.add_argument("--gib", type=float, default=0.0, help="input GiB of the chain/stream workloads (0 = 4 / 16)")
+    ap.add_argument("--jobs", type=int, default=160, help="jobs in the batched/served sample")
     return ap.parse_args(argv)
 
 
@@ -320,6 +329,10 @@ def run_ours(args, dist: Dist):
     if not args.no_e2e:
         e2e = run_e2e(args, lib, n_run, rand_np, dist, dev, sel)
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args, lib)
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         cb, ct, desc = cpu_sample(rand_np, min(args.scale, 1.0))
@@ -350,12 +363,78 @@ def run_ours(args, dist: Dist):
         }
         if e2e:
             line["e2e"] = e2e
+        if batched:
+            line["batched"] = batched
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
     del outs, d_run, d_rand
     dist.close()
     return 0
+
+
+def run_batched(args, lib):
+    """Batched/served jobs: a sample of the 10,000-job workload (same generator: sizes
+    log-uniform 4 KiB-64 MiB, per-job alphabets of 4-64 symbols, 1-16 pairs with pattern 1-32 B
+    and replacement 0-64 B), through the request loop (cuda_replace_server_*) against the same
+    jobs issued one by one as plain unified() calls (one call per pair). Closed loop (all jobs
+    submitted at once) for jobs/s, then Poisson arrivals at half that rate for latency."""
+    import random
+
+    from cuda_replace_b200 import workloads as WL
+    from cuda_replace_b200.cuda_replace_wrapper import Server
+
+    jobs = [WL.c5_job(i) for i in range(args.jobs)]
+    n_bytes = sum(len(j.data) for j in jobs)
+    out = {"jobs": len(jobs), "input_bytes": n_bytes}
+    with Server(lib) as srv:
+        for j in jobs[:4]:  # warm-up: tuning, graphs, staging
+            srv.wait(srv.submit(j.data, j.pairs))
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        tickets = [srv.submit(j.data, j.pairs) for j in jobs]
+        outs = [srv.wait(t) for t in tickets]
+        secs = time.perf_counter() - t0
+        st = srv.stats()
+        rate = len(jobs) / secs
+        out.update({"jobs_per_s": round(rate, 2), "gbs_in": round(n_bytes / secs / 1e9, 3),
+                    "closed_loop_p50_ms": round(st["p50_us"] / 1e3, 3), "closed_loop_p99_ms": round(st["p99_us"] / 1e3, 3),
+                    "batches": st["batches"], "jobs_via_session": st["jobs_via_session"],
+                    "tile_bytes": st["tile_bytes"], "grid_ctas": st["grid_ctas"]})
+        # open loop: Poisson arrivals at half the closed-loop rate
+        lam = 0.5 * rate
+        rng = random.Random(5)
+        srv.reset_stats()
+        t_start = time.perf_counter()
+        t_next = t_start
+        tickets = []
+        for j in jobs:
+            t_next += rng.expovariate(lam)
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(j.data, j.pairs))
+        for t in tickets:
+            srv.wait(t)
+        st = srv.stats()
+        out.update({"poisson_rate_jobs_per_s": round(lam, 2), "p50_ms": round(st["p50_us"] / 1e3, 3),
+                    "p99_ms": round(st["p99_us"] / 1e3, 3)})
+    # per-job plain unified() on a prefix of the same jobs
+    m = min(len(jobs), max(8, len(jobs) // 6))
+    t0 = time.perf_counter()
+    base = []
+    for j in jobs[:m]:
+        d = j.data
+        for p, r in j.pairs:
+            d = lib.unified(d, p, r)
+        base.append(d)
+    ub = time.perf_counter() - t0
+    if any(outs[i] != base[i] for i in range(m)):
+        raise SystemExit("batched self-check failed: results differ from per-job unified()")
+    out["unified_jobs_per_s"] = round(m / ub, 2)
+    out["unified_sample_jobs"] = m
+    out["speedup_vs_unified"] = round(rate / (m / ub), 2)
+    return out
 
 
 def run_e2e(args, lib, n_run, rand_np, dist: Dist, dev, sel):
@@ -398,11 +477,97 @@ def run_e2e(args, lib, n_run, rand_np, dist: Dist, dev, sel):
             "steps": steps, "api": "cuda_replace_unified (page-locked host input)"}
 
 
+def tiled_text(total: int, seed: int):
+    """total bytes of the Zipf text generator: a 256 MiB generated block repeated (generating
+    16 GiB directly would take minutes)."""
+    from cuda_replace_b200 import workloads as WL
+    base = WL.text_corpus(min(total, 256 * MiB), seed=seed)
+    reps = total // len(base) + 1
+    return (base * reps)[:total]
+
+
+def run_chain(args):
+    """4 GiB text, 128 entity pairs applied in order with Session.apply_batch (lengths chained
+    on the device). Metric: GB/s of sum over passes of (input + output) bytes, input resident."""
+    from cuda_replace_b200 import workloads as WL
+    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib, Session
+    lib = CudaReplaceLib()
+    total = int((args.gib or 4.0) * GiB)
+    txt = tiled_text(total, seed=3)
+    pairs = WL.c3_pairs(seed=3)
+    with Session(lib, txt) as s:
+        lens = [len(txt)]
+        for p, r in pairs:  # pass lengths, for the algorithmic bytes
+            lens.append(s.apply(p, r))
+        algo = sum(lens[k] + lens[k + 1] for k in range(len(pairs)))
+        times = []
+        for it in range(max(args.warmup, 1) + max(args.steps, 1)):
+            s.reset(txt)
+            t0 = time.perf_counter()
+            n = s.apply_batch(pairs)
+            dt = time.perf_counter() - t0
+            if n != lens[-1]:
+                raise SystemExit(f"chain self-check failed: {n} != {lens[-1]}")
+            if it >= max(args.warmup, 1):
+                times.append(dt)
+        _, launches = s.stats()
+    t = statistics.median(times)
+    line = {"metric": "GB/s (sum over passes of in+out), 128-pair chain", "value": round(algo / t / 1e9, 2),
+            "unit": "GB/s", "n_gpus": 1, "steps": len(times), "warmup": max(args.warmup, 1),
+            "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "dtype": "u8",
+            "data": "synthetic (Zipf text, 256 MiB generated block repeated)",
+            "config": {"workload": f"{total / GiB:g} GiB text x 128 entity pairs, Session.apply_batch",
+                       "end_to_end_gbs": round((lens[0] + lens[-1]) / t / 1e9, 3), "final_len": lens[-1]},
+            "gpu_launches_per_step": len(pairs)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_stream(args):
+    """16 GiB text, 8 pairs (L 2-16, R 0-32), 256 MiB chunks, matches planted across every chunk
+    boundary, through gpu_replace_streaming (chunk-major: one host-link crossing each way)."""
+    from cuda_replace_b200 import workloads as WL
+    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib, gpu_replace_streaming
+    lib = CudaReplaceLib()
+    total = int((args.gib or 16.0) * GiB)
+    chunk = 256 * MiB
+    txt = tiled_text(total, seed=4)
+    pairs = WL.c4_pairs(seed=4)
+    planted = 0
+    for pat, _ in pairs[:4]:
+        txt, c = WL.plant_across_boundaries(txt, pat, chunk, seed=len(pat))
+        planted += c
+    times = []
+    out_len = 0
+    for it in range(1 + max(args.steps, 1)):
+        t0 = time.perf_counter()
+        out = gpu_replace_streaming(lib, txt, pairs, chunk_bytes=chunk)
+        dt = time.perf_counter() - t0
+        out_len = len(out)
+        del out
+        if it >= 1:
+            times.append(dt)
+    t = statistics.median(times)
+    line = {"metric": "GB/s of input, 8-pair streaming (host bytes in, host bytes out)",
+            "value": round(total / t / 1e9, 3), "unit": "GB/s", "n_gpus": 1, "steps": len(times), "warmup": 1,
+            "ms_per_step": round(t * 1e3, 1), "higher_is_better": True, "dtype": "u8",
+            "data": "synthetic (Zipf text, 256 MiB generated block repeated, matches planted at every chunk boundary)",
+            "config": {"workload": f"{total / GiB:g} GiB text x 8 pairs, chunk 256 MiB", "planted": planted,
+                       "h2d_bytes": total, "d2h_bytes": out_len,
+                       "host_link_gbs": round((total + out_len) / t / 1e9, 3)}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     dist = Dist()
     if args.impl == "reference":
         return run_reference(args, dist)
+    if args.workload == "chain":
+        return run_chain(args)
+    if args.workload == "stream":
+        return run_stream(args)
     return run_ours(args, dist)
 
 

@@ -668,6 +668,10 @@ void cache_give(Session* s) {
 
 CR_EXPORT const char* cuda_replace_version(void) { return "cuda_replace_b200 1.0 sm_100a single-pass look-back"; }
 
+CR_EXPORT void cuda_replace_host_copy(void* dst, const void* src, size_t n) {
+  if (dst && src && n) crb::parallel_memcpy(dst, src, n);
+}
+
 CR_EXPORT void cuda_free_host(void* p) {
   if (p) crb::host_free(p);
 }

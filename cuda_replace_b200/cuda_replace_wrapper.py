@@ -31,13 +31,44 @@ c_size_t_p = C.POINTER(c_size_t)
 c_uint8_pp = C.POINTER(c_uint8_p)
 
 
-def _bytes_at(ptr, n: int) -> bytes:
-    """Copy n bytes of library-owned memory into a bytes object (ctypes.string_at takes a
-    C int size, which results of 2 GiB and more overflow)."""
+_new_bytes = C.pythonapi.PyBytes_FromStringAndSize
+_new_bytes.restype = C.py_object
+_new_bytes.argtypes = [C.c_void_p, C.c_ssize_t]
+_bytes_buffer = C.pythonapi.PyBytes_AsString
+_bytes_buffer.restype = C.c_void_p
+_bytes_buffer.argtypes = [C.py_object]
+_PARALLEL_COPY_MIN = 4 << 20
+
+
+def _bytes_at(ptr, n: int, lib: Optional[C.CDLL] = None) -> bytes:
+    """Copy n bytes of library-owned memory into a new bytes object. Large results are copied
+    by the library on several host threads into a bytes object created uninitialised (the
+    page faults of fresh memory, not the copy, bound a single-threaded copy); ctypes.string_at
+    is not used because its size is a C int, which results of 2 GiB and more overflow."""
     if not n:
         return b""
     addr = C.cast(ptr, c_void_p).value
-    return memoryview((C.c_uint8 * n).from_address(addr)).cast("B").tobytes()
+    copy = getattr(lib, "cuda_replace_host_copy", None) if lib is not None else None
+    if copy is None or n < _PARALLEL_COPY_MIN:
+        return memoryview((C.c_uint8 * n).from_address(addr)).cast("B").tobytes()
+    out = _new_bytes(None, n)  # uninitialised, filled below before anyone else sees it
+    copy(c_void_p(_bytes_buffer(out)), c_void_p(addr), c_size_t(n))
+    return out
+
+
+def _src_pointer(src):
+    """(keep-alive object, pointer, length) of a bytes-like input without copying bytes objects."""
+    if isinstance(src, bytes):
+        return src, (C.cast(C.c_char_p(src), c_uint8_p) if src else c_uint8_p()), len(src)
+    mv = memoryview(src)
+    n = mv.nbytes
+    if not n:
+        return None, c_uint8_p(), 0
+    if mv.readonly:
+        b = bytes(mv)
+        return b, C.cast(C.c_char_p(b), c_uint8_p), n
+    holder = (C.c_uint8 * n).from_buffer(mv)
+    return holder, C.cast(holder, c_uint8_p), n
 
 
 def _bind(lib: C.CDLL, name: str, argtypes, restype, optional: bool = False) -> None:
@@ -116,6 +147,7 @@ class CudaReplaceLib:
         _bind(lib, "cuda_replace_jobs",
               [C.c_int, c_uint8_pp, c_size_t_p, c_int_p, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p,
                c_uint8_pp, c_size_t_p], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_host_copy", [c_void_p, c_void_p, c_size_t], None, optional=True)
         _bind(lib, "cuda_replace_stream",
               [c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t,
                C.POINTER(c_uint8_p), c_size_t_p], C.c_int, optional=True)
@@ -125,20 +157,21 @@ class CudaReplaceLib:
 
     def unified(self, src: bytes, pat: bytes, rep: bytes) -> bytes:
         """One-shot replace (reference: py:124-141)."""
-        src_buf = C.create_string_buffer(src, len(src) or 1)
+        keep, src_p, n = _src_pointer(src)
         pat_buf = C.create_string_buffer(pat, len(pat) or 1)
         rep_buf = C.create_string_buffer(rep, len(rep) or 1)
         out_ptr = c_uint8_p()
         out_len = c_size_t()
         rc = self.lib.cuda_replace_unified(
-            C.cast(src_buf, c_uint8_p), c_size_t(len(src)),
+            src_p, c_size_t(n),
             C.cast(pat_buf, c_uint8_p), C.c_int(len(pat)),
             C.cast(rep_buf, c_uint8_p), C.c_int(len(rep)),
             C.byref(out_ptr), C.byref(out_len))
+        del keep
         if rc != 0:
             raise RuntimeError(f"cuda_replace_unified failed rc={rc}")
         try:
-            return _bytes_at(out_ptr, out_len.value)
+            return _bytes_at(out_ptr, out_len.value, self.lib)
         finally:
             self.lib.cuda_free_host(out_ptr)
 
@@ -149,8 +182,9 @@ class Session:
     def __init__(self, lib: CudaReplaceLib, src: bytes):
         self.lib = lib
         self.h = c_void_p()
-        buf = C.create_string_buffer(src, len(src) or 1)
-        rc = lib.lib.cuda_replace_open(C.byref(self.h), C.cast(buf, c_uint8_p), c_size_t(len(src)))
+        keep, src_p, n = _src_pointer(src)
+        rc = lib.lib.cuda_replace_open(C.byref(self.h), src_p, c_size_t(n))
+        del keep
         if rc != 0:
             raise RuntimeError(f"cuda_replace_open failed rc={rc}")
 
@@ -161,8 +195,9 @@ class Session:
         self.close()
 
     def reset(self, src: bytes) -> None:
-        buf = C.create_string_buffer(src, len(src) or 1)
-        rc = self.lib.lib.cuda_replace_reset(self.h, C.cast(buf, c_uint8_p), c_size_t(len(src)))
+        keep, src_p, n = _src_pointer(src)
+        rc = self.lib.lib.cuda_replace_reset(self.h, src_p, c_size_t(n))
+        del keep
         if rc != 0:
             raise RuntimeError(f"cuda_replace_reset failed rc={rc}")
 
@@ -235,7 +270,7 @@ class Session:
         if rc != 0:
             raise RuntimeError(f"cuda_replace_result failed rc={rc}")
         try:
-            return _bytes_at(out_ptr, out_len.value)
+            return _bytes_at(out_ptr, out_len.value, self.lib.lib)
         finally:
             self.lib.lib.cuda_free_host(out_ptr)
 
@@ -304,16 +339,7 @@ class Server:
 
     def submit(self, data, pairs: Sequence[Tuple[bytes, bytes]]) -> int:
         keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(pairs)
-        mv = memoryview(data)
-        n = mv.nbytes
-        if not n:
-            holder, src_ptr = None, c_uint8_p()
-        elif isinstance(data, bytes) or mv.readonly:
-            holder = data if isinstance(data, bytes) else bytes(mv)
-            src_ptr = C.cast(C.c_char_p(holder), c_uint8_p)
-        else:
-            holder = (C.c_uint8 * n).from_buffer(mv)
-            src_ptr = C.cast(holder, c_uint8_p)
+        holder, src_ptr, n = _src_pointer(data)
         ticket = C.c_ulonglong(0)
         rc = self.lib.lib.cuda_replace_server_submit(
             self.h, src_ptr, c_size_t(n), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
@@ -334,7 +360,7 @@ class Server:
         if rc != 0:
             raise RuntimeError(f"cuda_replace_server_wait failed rc={rc}")
         try:
-            return _bytes_at(out_ptr, out_len.value)
+            return _bytes_at(out_ptr, out_len.value, self.lib.lib)
         finally:
             self.lib.lib.cuda_free_host(out_ptr)
 
@@ -386,7 +412,7 @@ def replace_jobs(lib: CudaReplaceLib, jobs: Sequence[Tuple[bytes, Sequence[Tuple
         raise RuntimeError(f"cuda_replace_jobs failed rc={rc}")
     res = []
     for i in range(nj):
-        res.append(_bytes_at(outs[i], out_lens[i]))
+        res.append(_bytes_at(outs[i], out_lens[i], lib.lib))
         lib.lib.cuda_free_host(outs[i])
     return res
 
@@ -433,16 +459,7 @@ def stream_native(lib: CudaReplaceLib, src, pairs: Sequence[Tuple[bytes, bytes]]
     if fn is None:
         return None
     keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(pairs)
-    mv = memoryview(src)
-    n = mv.nbytes
-    if not n:
-        holder, src_ptr = None, c_uint8_p()
-    elif isinstance(src, bytes) or mv.readonly:
-        holder = src if isinstance(src, bytes) else bytes(mv)
-        src_ptr = C.cast(C.c_char_p(holder), c_uint8_p)  # points into the bytes object: no copy
-    else:
-        holder = (C.c_uint8 * n).from_buffer(mv)
-        src_ptr = C.cast(holder, c_uint8_p)
+    holder, src_ptr, n = _src_pointer(src)
     out_ptr = c_uint8_p()
     out_len = c_size_t()
     rc = fn(src_ptr, c_size_t(n), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
@@ -454,7 +471,7 @@ def stream_native(lib: CudaReplaceLib, src, pairs: Sequence[Tuple[bytes, bytes]]
     if rc != 0:
         raise RuntimeError(f"cuda_replace_stream failed rc={rc}")
     try:
-        return _bytes_at(out_ptr, out_len.value)
+        return _bytes_at(out_ptr, out_len.value, lib.lib)
     finally:
         lib.lib.cuda_free_host(out_ptr)
 

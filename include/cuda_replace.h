@@ -182,6 +182,12 @@ int cuda_replace_stream(const uint8_t* src, size_t n, const uint8_t** pats, cons
                         const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
                         uint8_t** out_host, size_t* out_len);
 
+/* Host memcpy on up to 8 threads (large copies): moves a result out of the page-locked
+ * block the library returned into memory the caller allocated (in Python: a bytes object
+ * created uninitialised), whose first-touch page faults bound a single-threaded copy. No
+ * counterpart in the reference. */
+void cuda_replace_host_copy(void* dst, const void* src, size_t n);
+
 /* ---- Batched jobs and serving. No counterpart in the reference, whose only batch is the
  * sequential pair chain of one buffer (cuda_replace_apply_batch, cu:2465); a caller with many
  * independent buffers there makes one unified() call per buffer and pair

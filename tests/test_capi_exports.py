@@ -49,3 +49,16 @@ def test_library_is_built_for_sm100a():
     assert B.ARCH_FLAGS == ["-gencode", "arch=compute_100a,code=sm_100a"]
     lib = ctypes.CDLL(str(B.LIB_PATH))
     assert lib.cuda_replace_open is not None
+
+
+def test_host_copy_fills_new_bytes(cr_lib):
+    """cuda_replace_host_copy is plain host memory work (no GPU): large results are copied
+    into an uninitialised bytes object on several threads."""
+    import random
+    from cuda_replace_b200 import cuda_replace_wrapper as Wr
+    n = (9 << 20) + 12345
+    src = (ctypes.c_uint8 * n).from_buffer(bytearray(random.Random(1).randbytes(n)))
+    out = Wr._bytes_at(ctypes.cast(src, Wr.c_uint8_p), n, cr_lib.lib)
+    assert isinstance(out, bytes) and out == bytes(src)
+    small = Wr._bytes_at(ctypes.cast(src, Wr.c_uint8_p), 1000, cr_lib.lib)
+    assert small == bytes(src)[:1000]
