@@ -175,6 +175,7 @@ std::map<int, Tuning> g_tuning;  // by device
 struct Slot {
   cudaStream_t st = nullptr;
   cudaEvent_t ev_meta = nullptr;
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // batch start / rounds done (timing)
   int max_jobs = 0;
   SegJob* d_jobs = nullptr;  // [kMaxRounds][kClasses][max_jobs]
   SegJob* h_jobs = nullptr;
@@ -271,6 +272,8 @@ struct Slot {
     const size_t tables = (size_t)kMaxRounds * kClasses * max_jobs;
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_meta, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev_t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev_t1);
     if (e == cudaSuccess) e = cudaMalloc(&d_jobs, tables * sizeof(SegJob));
     if (e == cudaSuccess) e = cudaMallocHost(&h_jobs, tables * sizeof(SegJob));
     if (e == cudaSuccess) e = cudaMalloc(&d_njobs, kMaxRounds * kClasses * sizeof(unsigned int));
@@ -296,6 +299,8 @@ struct Slot {
     for (void* q : {(void*)h_jobs, (void*)h_njobs, (void*)h_pairs, (void*)h_res, (void*)h_lens})
       if (q) cudaFreeHost(q);
     if (ev_meta) cudaEventDestroy(ev_meta);
+    if (ev_t0) cudaEventDestroy(ev_t0);
+    if (ev_t1) cudaEventDestroy(ev_t1);
     if (st) cudaStreamDestroy(st);
     st = nullptr;
   }
@@ -319,6 +324,8 @@ class Engine {
     return p ? p : static_cast<uint8_t*>(crb::host_pinned_pool().get(n, e));
   }
   std::atomic<unsigned long long> seg_launches{0}, graph_launches{0};
+  // uploads + rounds on the device; result downloads (host wall), in microseconds
+  std::atomic<unsigned long long> gpu_us{0}, download_us{0};
 
   cudaError_t init(size_t budget, int mj) {
     cudaGetDevice(&device);
@@ -411,6 +418,7 @@ class Engine {
       }
     }
     // uploads: inputs, lengths, pairs, job tables, counts; results cleared
+    e = cudaEventRecord(s.ev_t0, s.st);
     for (int i = 0; i < nj && e == cudaSuccess; ++i) {
       Job& j = *batch[(size_t)i];
       if (j.n) e = cudaMemcpyAsync(base + j.off_in, j.hin, j.n, cudaMemcpyHostToDevice, s.st);
@@ -437,6 +445,8 @@ class Engine {
       e = run_rounds(s, rounds);
       if (e != cudaSuccess) return e;
     }
+    e = cudaEventRecord(s.ev_t1, s.st);
+    if (e != cudaSuccess) return e;
     // lengths and flags back
     e = cudaMemcpyAsync(s.h_lens, s.d_lens, (size_t)nj * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s.st);
     if (e == cudaSuccess)
@@ -479,6 +489,9 @@ class Engine {
   cudaError_t finish(Slot& s, std::vector<Job*>* rerun) {
     cudaError_t e = cudaEventSynchronize(s.ev_meta);
     if (e != cudaSuccess) return e;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, s.ev_t0, s.ev_t1) == cudaSuccess) gpu_us += (unsigned long long)(ms * 1000.0f);
+    const double t_dl = now_us();
     uint8_t* base = arena.base();
     const int nj = (int)s.jobs.size();
     for (int i = 0; i < nj && e == cudaSuccess; ++i) {
@@ -499,6 +512,7 @@ class Engine {
       }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s.st);
+    download_us += (unsigned long long)(now_us() - t_dl);
     return e;
   }
 
@@ -748,6 +762,9 @@ class Server {
     st->pending = (unsigned long long)(pending_.size() + fallback_q_.size());
     st->arena_bytes = eng_.arena.size();
     st->arena_peak_bytes = arena_peak_;
+    st->gpu_us = (double)eng_.gpu_us.load();
+    st->download_us = (double)eng_.download_us.load();
+    st->session_us = session_us_;
     std::vector<double> l = lat_;
     if (!l.empty()) {
       std::sort(l.begin(), l.end());
@@ -766,6 +783,9 @@ class Server {
     std::lock_guard<std::mutex> g(mu_);
     lat_.clear();
     jobs_done_ = jobs_session_ = batches_ = bytes_in_ = bytes_out_ = 0;
+    session_us_ = 0;
+    eng_.gpu_us = 0;
+    eng_.download_us = 0;
   }
 
  private:
@@ -891,9 +911,12 @@ class Server {
         crb::host_free(j->hout);
         j->hout = nullptr;
       }
+      const double t0 = now_us();
       const int rc = run_with_session(*j);
+      const double dt = now_us() - t0;
       mark_done(j, rc);
       lk.lock();
+      session_us_ += dt;
       running_fallback_ = false;
       cv_.notify_all();
     }
@@ -914,6 +937,7 @@ class Server {
   std::vector<double> lat_;
   unsigned long long jobs_done_ = 0, jobs_session_ = 0, batches_ = 0, bytes_in_ = 0, bytes_out_ = 0;
   unsigned long long arena_peak_ = 0;
+  double session_us_ = 0;
 };
 
 size_t default_budget() {

@@ -276,12 +276,51 @@ int session_create(Session** out) {
 }
 
 // Upload src[0, len) into the session buffer.
+bool host_is_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Host -> device copy of len bytes. A large pageable source is staged through two page-locked
+// 32 MiB buffers filled by several host threads, so the copy runs near the host link's speed
+// (a pageable cudaMemcpy goes through the driver's single-threaded staging).
+cudaError_t upload_host(uint8_t* dst, const uint8_t* src, size_t len, cudaStream_t st) {
+  const size_t kChunk = 32u << 20;
+  if (len < (8u << 20) || host_is_pinned(src)) return cudaMemcpyAsync(dst, src, len, cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaSuccess;
+  uint8_t* stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    stage[b] = static_cast<uint8_t*>(pinned_pool().get(kChunk, &e));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+  }
+  for (size_t off = 0, i = 0; off < len && e == cudaSuccess; off += kChunk, ++i) {
+    const int b = (int)(i & 1);
+    const size_t m = std::min(kChunk, len - off);
+    if (i >= 2) e = cudaEventSynchronize(ev[b]);  // stage[b] has reached the device
+    if (e != cudaSuccess) break;
+    crb::parallel_memcpy(stage[b], src + off, m);
+    e = cudaMemcpyAsync(dst + off, stage[b], m, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[b], st);
+  }
+  const cudaError_t se = cudaStreamSynchronize(st);  // the staging goes back to the pool
+  for (int b = 0; b < 2; ++b) {
+    if (ev[b]) cudaEventDestroy(ev[b]);
+    if (stage[b]) pinned_pool().put(stage[b]);
+  }
+  return e != cudaSuccess ? e : se;
+}
+
 int session_load(Session* s, const uint8_t* src, size_t len) {
   if (len && !src) return -1;
   cudaError_t e = dev_grow(&s->buf, &s->buf_cap, len ? len : 1, false, 0, s->stream);
   if (e != cudaSuccess) return (int)e;
   if (len) {
-    e = cudaMemcpyAsync(s->buf, src, len, cudaMemcpyHostToDevice, s->stream);
+    e = upload_host(s->buf, src, len, s->stream);
     if (e != cudaSuccess) return (int)e;
   }
   e = cudaStreamSynchronize(s->stream);

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <condition_variable>
 #include <cstring>
 #include <iterator>
 #include <map>
@@ -76,26 +77,78 @@ class PinnedPool {
 // The process-wide pool (never destroyed: CUDA may be torn down first at exit).
 PinnedPool& host_pinned_pool();
 
-// memcpy split over up to 8 host threads when it is large (pageable <-> page-locked staging).
-inline void parallel_memcpy(void* dst, const void* src, size_t n) {
-  const size_t kMin = 8u << 20;
-  const unsigned hw = std::thread::hardware_concurrency();
-  const unsigned t = hw ? (hw < 8u ? hw : 8u) : 4u;
-  if (n < kMin || t < 2) {
-    memcpy(dst, src, n);
-    return;
+// A few persistent host threads for large memcpys (pageable <-> page-locked staging, result
+// copies): spawning threads per copy would cost more than the copy of a 32 MiB chunk.
+class CopyWorkers {
+ public:
+  static CopyWorkers& get() {
+    static CopyWorkers* w = new CopyWorkers();  // never destroyed (threads parked at exit)
+    return *w;
   }
-  const size_t part = pool_round_up((n + t - 1) / t, 4096);
-  std::vector<std::thread> th;
-  for (unsigned i = 1; i < t; ++i) {
-    const size_t a = part * i;
-    if (a >= n) break;
-    const size_t len = part < n - a ? part : n - a;
-    th.emplace_back([=]() { memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, len); });
+  // dst[0, n) = src[0, n), split across the workers and the calling thread
+  void copy(void* dst, const void* src, size_t n) {
+    const size_t kMin = 8u << 20;
+    const unsigned parts = nthreads_ + 1;
+    if (n < kMin || nthreads_ == 0) {
+      memcpy(dst, src, n);
+      return;
+    }
+    const size_t part = pool_round_up((n + parts - 1) / parts, 4096);
+    std::unique_lock<std::mutex> lk(mu_);
+    caller_.wait(lk, [&] { return !busy_; });  // one parallel copy at a time
+    busy_ = true;
+    dst_ = static_cast<char*>(dst);
+    src_ = static_cast<const char*>(src);
+    n_ = n;
+    part_ = part;
+    next_ = 1;  // part 0 is the caller's
+    pending_ = 0;
+    for (unsigned i = 1; i < parts; ++i)
+      if (part * i < n) ++pending_;
+    ++gen_;
+    work_.notify_all();
+    lk.unlock();
+    memcpy(dst, src, part < n ? part : n);
+    lk.lock();
+    done_.wait(lk, [&] { return pending_ == 0; });
+    busy_ = false;
+    caller_.notify_one();
   }
-  memcpy(dst, src, part < n ? part : n);
-  for (auto& x : th) x.join();
-}
+
+ private:
+  CopyWorkers() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    nthreads_ = hw > 1 ? (hw - 1 < 7u ? hw - 1 : 7u) : 0u;
+    for (unsigned i = 0; i < nthreads_; ++i) std::thread([this] { loop(); }).detach();
+  }
+  void loop() {
+    unsigned long long seen = 0;
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      work_.wait(lk, [&] { return gen_ != seen && busy_ && next_ * part_ < n_; });
+      const size_t i = next_++;
+      if (next_ * part_ >= n_ || next_ > nthreads_) seen = gen_;
+      char* d = dst_;
+      const char* s = src_;
+      const size_t a = i * part_, len = part_ < n_ - a ? part_ : n_ - a;
+      lk.unlock();
+      memcpy(d + a, s + a, len);
+      lk.lock();
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  std::mutex mu_;
+  std::condition_variable work_, done_, caller_;
+  unsigned nthreads_ = 0;
+  bool busy_ = false;
+  char* dst_ = nullptr;
+  const char* src_ = nullptr;
+  size_t n_ = 0, part_ = 0, next_ = 0, pending_ = 0;
+  unsigned long long gen_ = 0;
+};
+
+// memcpy split over the copy workers when it is large.
+inline void parallel_memcpy(void* dst, const void* src, size_t n) { CopyWorkers::get().copy(dst, src, n); }
 
 // First-fit sub-allocator over one page-locked block: a server's host staging area, pinned
 // once instead of per request. Blocks handed to callers are released with cuda_free_host

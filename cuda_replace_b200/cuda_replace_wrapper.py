@@ -86,7 +86,8 @@ class ServerStats(C.Structure):
                 ("bytes_in", C.c_ulonglong), ("bytes_out", C.c_ulonglong), ("kernel_launches", C.c_ulonglong),
                 ("graph_launches", C.c_ulonglong), ("pending", C.c_ulonglong), ("arena_bytes", C.c_ulonglong),
                 ("arena_peak_bytes", C.c_ulonglong), ("p50_us", C.c_double), ("p99_us", C.c_double),
-                ("max_us", C.c_double), ("tile_bytes", C.c_uint * 3), ("grid_ctas", C.c_int * 3)]
+                ("max_us", C.c_double), ("gpu_us", C.c_double), ("download_us", C.c_double),
+                ("session_us", C.c_double), ("tile_bytes", C.c_uint * 3), ("grid_ctas", C.c_int * 3)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}

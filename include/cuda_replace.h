@@ -216,6 +216,9 @@ typedef struct CudaReplaceServerStats {
   unsigned long long pending;           /* requests queued, not yet on the device */
   unsigned long long arena_bytes, arena_peak_bytes;
   double p50_us, p99_us, max_us;        /* latency: submit() to result ready */
+  double gpu_us;                        /* batches on the device: uploads and rounds (CUDA events) */
+  double download_us;                   /* result downloads, host wall time */
+  double session_us;                    /* jobs run through a Session, host wall time */
   unsigned int tile_bytes[3];           /* autotuned super-tile bytes: free, bordered L<=4, bordered L<=32 */
   int grid_ctas[3];
 } CudaReplaceServerStats;
