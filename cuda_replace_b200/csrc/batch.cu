@@ -139,21 +139,27 @@ struct Job {
   int rc = 0;
   bool done = false;
   bool via_session = false;
+  int retries = 0;           // segmented reruns after an overflow
   double t_submit = 0, t_done = 0;
 };
 
-// Output capacity of a job's ping-pong buffers: the worst case of its chain when that is at
-// most 4n + 1 MiB (no overflow possible), else 4n + 1 MiB (an overflow reruns the job).
-size_t job_capacity(const Job& j) {
-  const long double lim = 4.0L * (long double)j.n + (long double)(1u << 20);
+// Largest intermediate length of a job's chain in the worst case (every pattern position a
+// match), capped at `lim`.
+long double chain_worst(const Job& j, long double lim) {
   long double wc = (long double)j.n, mx = wc;
   for (const SegPair& q : j.seg) {
     if (q.R > q.L) wc += (long double)((unsigned long long)wc / q.L) * (long double)(q.R - q.L);
     mx = std::max(mx, wc);
     if (mx > lim) break;
   }
-  const long double c = std::min(mx, lim);
-  return rup((size_t)c + 16, kAlign);
+  return std::min(mx, lim);
+}
+
+// Output capacity of a job's ping-pong buffers: the worst case of its chain when that is at
+// most 4n + 1 MiB (no overflow possible), else 4n + 1 MiB (an overflow reruns the job).
+size_t job_capacity(const Job& j) {
+  const long double lim = 4.0L * (long double)j.n + (long double)(1u << 20);
+  return rup((size_t)chain_worst(j, lim) + 16, kAlign);
 }
 
 // ------------------------------------------------------------------ autotuning
@@ -333,7 +339,7 @@ class Engine {
     cudaError_t e = arena.init(budget);
     if (e == cudaSuccess) {
       hstage = new crb::HostArena();
-      e = hstage->init(std::min<size_t>(4ull << 30, std::max<size_t>(64u << 20, budget / 4)));
+      e = hstage->init(std::min<size_t>(8ull << 30, std::max<size_t>(64u << 20, budget / 4)));
       if (e != cudaSuccess) {
         delete hstage;
         hstage = nullptr;
@@ -499,6 +505,13 @@ class Engine {
       const ApplyResult& r = s.h_res[i];
       const int k = (int)j.seg.size();
       if (r.error_epoch != 0u || r.overflow_epoch != 0u) {
+        if (r.error_epoch == 0u) {
+          // overflow: the length that did not fit is in one of the two length slots
+          j.out_len = (size_t)std::max(s.h_lens[2 * i], s.h_lens[2 * i + 1]);
+        } else {
+          j.out_len = 0;
+          j.retries = 1 << 20;  // an error: no segmented rerun
+        }
         rerun->push_back(&j);
         continue;
       }
@@ -633,7 +646,7 @@ class Engine {
 // ------------------------------------------------------------------ Session path
 // A job outside the segmented limits, or one whose output outgrew its buffers, runs
 // through a Session (exact sizing), one pair at a time on the device.
-int run_with_session(Job& j) {
+int run_with_session(Job& j, Engine& eng) {
   void* h = nullptr;
   int rc = cuda_replace_open(&h, j.hin, j.n);
   if (rc != 0) return rc;
@@ -648,7 +661,15 @@ int run_with_session(Job& j) {
   }
   size_t nl = 0;
   if (k) rc = cuda_replace_apply_batch(h, pp.data(), pl.data(), rr.data(), rl.data(), k, &nl);
-  if (rc == 0) rc = cuda_replace_result(h, &j.hout, &j.out_len);
+  if (rc == 0) rc = cuda_replace_length(h, &nl);
+  if (rc == 0 && nl) {
+    cudaError_t e;
+    j.hout = eng.host_get(nl, &e);  // page-locked staging, not a fresh pinned block
+    if (!j.hout) rc = (int)e;
+    if (rc == 0) rc = cuda_replace_result_into(h, j.hout, nl, &j.out_len);
+  } else if (rc == 0) {
+    j.out_len = 0;
+  }
   cuda_replace_close(h);
   j.via_session = true;
   return rc;
@@ -889,7 +910,23 @@ class Server {
         if (std::find(rerun.begin(), rerun.end(), j) == rerun.end()) mark_done(j, e == cudaSuccess ? 0 : (int)e);
       lk.lock();
       for (Job* j : s.jobs) eng_.unplace(*j);
-      for (Job* j : rerun) fallback_q_.push_back(j);
+      // an overflowed job runs again, first in the queue, with buffers grown past the length
+      // that overflowed (at most twice); otherwise, and after an error, through a Session
+      for (auto it = rerun.rbegin(); it != rerun.rend(); ++it) {
+        Job* j = *it;
+        if (j->retries < 2) {
+          const long double need = (long double)j->out_len * 1.5L + (long double)(1u << 20);
+          const long double grown = std::max(need, 2.0L * (long double)j->cap);
+          j->cap = rup((size_t)std::min(grown, chain_worst(*j, grown)) + 16, kAlign);
+          ++j->retries;
+          j->out_len = 0;
+          if (Engine::footprint(*j) <= eng_.arena.size()) {
+            pending_.push_front(j);
+            continue;
+          }
+        }
+        fallback_q_.push_back(j);
+      }
       s.jobs.clear();
       s.busy = false;
       ++completions_;
@@ -912,7 +949,7 @@ class Server {
         j->hout = nullptr;
       }
       const double t0 = now_us();
-      const int rc = run_with_session(*j);
+      const int rc = run_with_session(*j, eng_);
       const double dt = now_us() - t0;
       mark_done(j, rc);
       lk.lock();

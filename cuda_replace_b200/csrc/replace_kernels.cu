@@ -831,8 +831,9 @@ __global__ void __launch_bounds__(kThreads) query_tile_kernel(const __grid_const
 // One CTA before every segmented launch: draw the launch's epoch (clearing the look-back
 // scratch when the 24-bit record tag or the 30-bit status epoch wraps), read every job's
 // input length, give each job its range of super-tiles and fill the super-tile -> job map.
-// A job whose result block holds an error or overflow epoch (an earlier launch of its chain
-// failed) or whose input is empty gets no super-tile and an empty output.
+// A job whose input is empty gets no super-tile and an empty output; a job whose result
+// block holds an error or overflow epoch (an earlier launch of its chain failed) gets no
+// super-tile and its lengths stay as they were (the host reads the length that overflowed).
 __global__ void __launch_bounds__(1024) seg_plan_kernel(const __grid_constant__ SegLaunch sl) {
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_epoch, s_clear;
@@ -871,7 +872,7 @@ __global__ void __launch_bounds__(1024) seg_plan_kernel(const __grid_constant__ 
       const unsigned long long n = failed ? 0ull : *J.n_dev;
       const unsigned long long t = (n + S - 1ull) / S;
       nt = t < 0xFFFFFFFFull ? (uint32_t)t : 0xFFFFFFFFu;
-      if (nt == 0) *J.len_out = 0;
+      if (nt == 0 && !failed) *J.len_out = 0;  // a failed job keeps the length that overflowed
     }
     // block exclusive scan of nt
     uint32_t x = nt;

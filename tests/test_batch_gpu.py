@@ -135,3 +135,18 @@ def test_server_wait_timeout_and_unknown_ticket(cr_lib):
         assert out == b"ac" * 1000
         with pytest.raises(RuntimeError, match="rc=-1"):
             srv.wait(t, timeout_ms=0)  # retired
+
+
+def test_server_overflow_reruns_segmented(cr_lib):
+    """Outputs far above the planned buffers (64x expansion) are flagged by the kernel without
+    writing out of range; the job runs again in a later batch with buffers grown past the
+    length that overflowed, not through a Session."""
+    jobs = [(b"a" * 100_000, [(b"a", b"Q" * 64)]),
+            (b"ab" * 300_000, [(b"b", b"R" * 60), (b"aR", b"S" * 64)]),
+            (b"xyz" * 1000, [(b"y", b"")])]
+    with Wr.Server(cr_lib, hbm_budget=512 << 20) as srv:
+        outs = [srv.wait(srv.submit(d, p)) for d, p in jobs]
+        st = srv.stats()
+    assert st["jobs_via_session"] == 0
+    for i, ((data, pairs), out) in enumerate(zip(jobs, outs)):
+        assert out == chain(data, pairs), i
