@@ -956,6 +956,7 @@ constexpr int kMaxSub = 8;
 
 struct LayoutS {
   uint32_t in0, outb, masks, pat, rep, tab16, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
+  uint32_t masks_set, srec_set, wtab_set, wrec_set, subrec_set;  // bytes of one set of per-super-tile tables
   uint32_t rs, inbytes;
   uint32_t wstage_words;  // padded staging words per warp (its 2 KiB of input may grow 3x)
 };
@@ -968,8 +969,10 @@ __host__ __device__ __forceinline__ uint32_t stage_ratio(uint32_t L, uint32_t R)
 }
 
 // ratio: output staging per input byte (0: from L and R; a segmented launch passes the largest).
+// sets: per-super-tile tables held at once (2 when one super-tile's pass A overlaps the
+// previous one's look-back and pass B).
 __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_t L, uint32_t R, uint32_t nsub,
-                                                          uint32_t ratio = 0) {
+                                                          uint32_t ratio = 0, uint32_t sets = 1) {
   LayoutS s{};
   uint32_t off = 0;
   s.inbytes = align_up_u32(kTile + (L > 1 ? L - 1 : 0), 16) + 32;
@@ -982,7 +985,8 @@ __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_
   s.outb = off;
   off += align_up_u32(kWarps * s.wstage_words * 4u, 16);
   s.masks = off;
-  off += nsub * kThreads * 8;
+  s.masks_set = nsub * kThreads * 8;
+  off += sets * s.masks_set;
   s.pat = off;
   off += align_up_u32(L ? L : 1, 16);
   s.rep = off;
@@ -996,13 +1000,17 @@ __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_
       off += align_up_u32(kThreads * s.rs * 2, 16);
     }
     s.srec = off;
-    off += align_up_u32(nsub * kThreads * L, 16);
+    s.srec_set = align_up_u32(nsub * kThreads * L, 16);
+    off += sets * s.srec_set;
     s.wtab = off;
-    off += align_up_u32(nsub * kWarps * L * 4, 16);
+    s.wtab_set = align_up_u32(nsub * kWarps * L * 4, 16);
+    off += sets * s.wtab_set;
     s.wrec = off;
-    off += align_up_u32(nsub * kWarps * L, 16);
+    s.wrec_set = align_up_u32(nsub * kWarps * L, 16);
+    off += sets * s.wrec_set;
     s.subrec = off;
-    off += align_up_u32(nsub * L, 16);
+    s.subrec_set = align_up_u32(nsub * L, 16);
+    off += sets * s.subrec_set;
   }
   s.total = off;
   return s;
@@ -1554,24 +1562,36 @@ __device__ __forceinline__ uint32_t subs_in_tile(uint32_t tile, unsigned long lo
 // `consumed` count; only thread 0 issues (and tracks the issue position).
 struct LoadRing {
   uint32_t issued, consumed;
-  uint32_t iq, iph, ij;  // next load: queue slot (0 current, 1 next super-tile), pass, sub-tile
+  uint32_t ij;                          // next sub-tile of the head phase
+  uint32_t nph;                         // phases queued (at most 2)
+  uint32_t ph_t0, ph_k0, ph_t1, ph_k1;  // queued phases: super-tile, kind (0: pass A, 1: pass B)
 
   __device__ __forceinline__ void init() {
     issued = consumed = 0;
-    iq = iph = ij = 0;
+    ij = nph = 0;
+    ph_t0 = ph_k0 = ph_t1 = ph_k1 = 0;
   }
-  __device__ __forceinline__ void issue(const ReplaceParams& p, uint8_t* smem, const LayoutS& lay,
-                                        uint64_t* bars, uint32_t* q, unsigned long long S,
-                                        unsigned long long n16, uint32_t want_a, unsigned long long n,
-                                        uint32_t NT) {
-    while (issued - consumed < (uint32_t)kNBuf) {
-      if (iq >= 1) break;  // loads of the next super-tile start once it is claimed
-      const uint32_t tile = q[iq];
-      if (tile >= NT) break;
-      const uint32_t m = subs_in_tile(tile, S, n, p.nsub);
-      const unsigned long long start = (unsigned long long)tile * S + (unsigned long long)ij * kTile;
+  // Thread 0: queue the loads of one pass over super-tile t (kind 0: sub-tiles with their
+  // halo, for pass A; kind 1: sub-tiles, for pass B), consumed in the order queued.
+  __device__ __forceinline__ void push(uint32_t t, uint32_t kind) {
+    if (nph == 0) {
+      ph_t0 = t;
+      ph_k0 = kind;
+    } else {
+      ph_t1 = t;
+      ph_k1 = kind;
+    }
+    ++nph;
+  }
+  // Thread 0: keep up to kNBuf loads in flight.
+  __device__ __forceinline__ void issue(const ReplaceParams& p, uint8_t* smem, const LayoutS& lay, uint64_t* bars,
+                                        unsigned long long S, unsigned long long n16, uint32_t want_a,
+                                        unsigned long long n, uint32_t nsub) {
+    while (issued - consumed < (uint32_t)kNBuf && nph > 0) {
+      const uint32_t m = subs_in_tile(ph_t0, S, n, nsub);
+      const unsigned long long start = (unsigned long long)ph_t0 * S + (unsigned long long)ij * kTile;
       const unsigned long long avail = n16 - start;
-      const uint32_t want = iph == 0 ? want_a : (uint32_t)kTile;
+      const uint32_t want = ph_k0 == 0 ? want_a : (uint32_t)kTile;
       const uint32_t bytes = avail < want ? (uint32_t)avail : want;
       const uint32_t b = issued % kNBuf;
       fence_proxy_async_smem();
@@ -1580,12 +1600,9 @@ struct LoadRing {
       ++issued;
       if (++ij == m) {
         ij = 0;
-        if (iph == 0) {
-          iph = 1;
-        } else {
-          iph = 0;
-          ++iq;
-        }
+        ph_t0 = ph_t1;
+        ph_k0 = ph_k1;
+        --nph;
       }
     }
   }
@@ -1603,7 +1620,6 @@ struct LoadRing {
     return smem + lay.in0 + b * lay.inbytes;
   }
   __device__ __forceinline__ void release() { ++consumed; }
-  __device__ __forceinline__ void shift() { iq = 0; iph = 0; ij = 0; }
 };
 
 // Input length, output range and super-tile count of the job described by p.
@@ -1689,14 +1705,20 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ uint32_t s_cin;
   __shared__ uint32_t s_fail;
   __shared__ uint32_t s_cutlen;             // exact output length of the warp region cut at n
-  __shared__ uint32_t s_sub_lco[kMaxSub];
-  __shared__ uint32_t s_wcnt[kMaxSub * kWarps];   // kModeFree: kept count per (sub-tile, warp)
-  __shared__ uint32_t s_wcend[kMaxSub * kWarps];  // kModeFree: max cover end per (sub-tile, warp)
+  // per-super-tile tables, two sets: one super-tile's pass A runs while the previous one
+  // looks back and writes its output (one set in a segmented launch)
+  __shared__ uint32_t s_sub_lco[2 * kMaxSub];
+  __shared__ uint32_t s_wcnt[2 * kMaxSub * kWarps];   // kModeFree: kept count per (sub-tile, warp)
+  __shared__ uint32_t s_wcend[2 * kMaxSub * kWarps];  // kModeFree: max cover end per (sub-tile, warp)
+  __shared__ unsigned long long s_frcnt[2];          // kModeFree: super-tile function (count, local carry-out)
+  __shared__ long long s_frlco[2];
+  __shared__ uint32_t s_supc[2][32], s_supx[2][32];  // kModeSmall: super-tile table over carries
 
   const ReplaceParams& p = SEG ? s_job : pk;
   unsigned int* const sched = SEG ? sl.sched : &pk.res->tile_counter;  // claim counter, then finished CTAs
   const uint32_t nsub = SEG ? sl.nsub : pk.nsub;
-  const LayoutS lay = SEG ? make_layout_s(MODE, sl.Lmax, sl.Rmax, nsub, 3u) : make_layout_s(MODE, pk.L, pk.R, nsub);
+  const LayoutS lay =
+      SEG ? make_layout_s(MODE, sl.Lmax, sl.Rmax, nsub, 3u) : make_layout_s(MODE, pk.L, pk.R, nsub, 0u, 2u);
   uint8_t* ps = smem + lay.pat;
   uint8_t* rs = smem + lay.rep;
   uint8_t* ob = smem + lay.outb;
@@ -1743,52 +1765,22 @@ __global__ void __launch_bounds__(kThreads, 3)
   }
   uint32_t nscan = 0;  // block_excl_scan1 calls so far (selects the scratch buffer)
 
-  // ---- load ring: thread 0 issues loads in the order they are consumed: for the current
-  // super-tile, pass A (sub-tile + halo) then pass B (sub-tile).
+  // ---- load ring: thread 0 queues the loads of each pass in the order they are consumed
   LoadRing ring;
   ring.init();
-  if (tid == 0) {
-    for (int b = 0; b < kNBuf; ++b) mbar_init(&s_bar[b], 1);
-    fence_mbar_init();
-    if (SEG) {
-      s_jobid = 0xFFFFFFFFu;
-      s_newjob = 0;
-      s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
-    } else {
-      const uint32_t first = atomicAdd(sched, 1u);
-      s_q[0] = first < NT ? first : NT;
-    }
-    s_q[1] = 0xFFFFFFFFu;
-    s_fail = 0;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    if (SEG) {
-      if (s_q[0] != 0xFFFFFFFFu) {
-        const JobDims d = job_dims(p, S);
-        ring.issue(p, smem, lay, s_bar, s_q, S, d.n16, d.want_a, d.n, d.NT);
-      }
-    } else {
-      ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
-    }
-  }
 
-  for (;;) {
-    __syncthreads();
-    const uint32_t t = s_q[0];
-    if (SEG) {
-      if (t == 0xFFFFFFFFu) break;
-      if (s_newjob) {  // a super-tile of another job: its dimensions and pattern
-        setup_job();
-        __syncthreads();
-        if (tid == 0) s_newjob = 0;
-      }
-    } else if (t >= NT) {
-      break;
-    }
+  // pass A of super-tile t and its function (published as an aggregate record); tables in set `set`
+  auto tile_front = [&](const uint32_t t, const uint32_t set) {
     const uint32_t m = subs_in_tile(t, S, n, nsub);
     const unsigned long long tstart = (unsigned long long)t * S;
-
+    uint64_t* const masks_s = masks + (size_t)set * nsub * kThreads;
+    uint32_t* const wcnt_s = s_wcnt + set * (kMaxSub * kWarps);
+    uint32_t* const wcend_s = s_wcend + set * (kMaxSub * kWarps);
+    uint32_t* const sublco_s = s_sub_lco + set * kMaxSub;
+    uint8_t* const srec_b = smem + lay.srec + set * lay.srec_set;
+    uint8_t* const wtab_b = smem + lay.wtab + set * lay.wtab_set;
+    uint8_t* const wrec_b = smem + lay.wrec + set * lay.wrec_set;
+    uint8_t* const subrec_b = smem + lay.subrec + set * lay.subrec_set;
     // ================= pass A: candidates and per-warp functions of every sub-tile
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
@@ -1810,7 +1802,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         mask &= low_bits(hi) & ~low_bits(lo);
       }
       if (L > 4) mask = verify_tail(mask, tb + sb, ps, L);
-      masks[j * kThreads + tid] = mask;
+      masks_s[j * kThreads + tid] = mask;
       if (MODE == kModeFree) {
         // every candidate is kept: per warp, the count and how far its last match reaches
         uint32_t cnt = (uint32_t)__popcll(mask);
@@ -1822,12 +1814,12 @@ __global__ void __launch_bounds__(kThreads, 3)
           cend = o > cend ? o : cend;
         }
         if (lane == 0) {
-          s_wcnt[j * kWarps + warp] = cnt;
-          s_wcend[j * kWarps + warp] = cend;
+          wcnt_s[j * kWarps + warp] = cnt;
+          wcend_s[j * kWarps + warp] = cend;
         }
       } else {
-        uint8_t* srec = smem + lay.srec + (size_t)j * kThreads * L;
-        uint32_t* wtab = reinterpret_cast<uint32_t*>(smem + lay.wtab) + (size_t)(j * kWarps + warp) * L;
+        uint8_t* srec = srec_b + (size_t)j * kThreads * L;
+        uint32_t* wtab = reinterpret_cast<uint32_t*>(wtab_b) + (size_t)(j * kWarps + warp) * L;
         if (L == 2u) {
           ks_warp_tables<2>(mask, p.inv_l, p.stride_mask, srec + tid * 2u, wtab);
         } else if (L == 3u) {
@@ -1857,7 +1849,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       __syncthreads();
       ring.release();
-      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
     }
 
     // ================= fold the sub-tiles into the super-tile function
@@ -1871,12 +1863,12 @@ __global__ void __launch_bounds__(kThreads, 3)
         for (uint32_t j = 0; j < m; ++j) {
           uint32_t tot_cnt = 0, tot_cend = 0;
           for (int w = 0; w < kWarps; ++w) {
-            tot_cnt += s_wcnt[j * kWarps + w];
-            const uint32_t ce = s_wcend[j * kWarps + w];
+            tot_cnt += wcnt_s[j * kWarps + w];
+            const uint32_t ce = wcend_s[j * kWarps + w];
             tot_cend = ce > tot_cend ? ce : tot_cend;
           }
           const long long lco = tot_cend > (uint32_t)kTile ? (long long)(tot_cend - kTile) : 0ll;
-          s_sub_lco[j] = (uint32_t)lco;
+          sublco_s[j] = (uint32_t)lco;
           const long long shifted = fr_lco - (long long)kTile;
           fr_lco = shifted > lco ? shifted : lco;
           fr_cnt += tot_cnt;
@@ -1885,9 +1877,9 @@ __global__ void __launch_bounds__(kThreads, 3)
           rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
       }
     } else if (warp == 0) {
-      const uint32_t* wt = reinterpret_cast<const uint32_t*>(smem + lay.wtab);
+      const uint32_t* wt = reinterpret_cast<const uint32_t*>(wtab_b);
       for (uint32_t j = 0; j < m; ++j) {
-        uint8_t* wrec = smem + lay.wrec + (size_t)j * kWarps * L;
+        uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
         uint32_t y = lane < L ? lane : 0u, cnt = 0;
 #pragma unroll
         for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
@@ -1896,7 +1888,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           cnt += v & 0xFFFFu;
           y = v >> 16;
         }
-        if (lane < L) (smem + lay.subrec)[j * L + lane] = (uint8_t)sup_carry;
+        if (lane < L) (subrec_b)[j * L + lane] = (uint8_t)sup_carry;
         const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
         const uint32_t tx = __shfl_sync(0xffffffffu, y, sup_carry);
         sup_cnt += tc;
@@ -1918,6 +1910,31 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
 
+    if (MODE == kModeFree) {
+      if (tid == 0) {
+        s_frcnt[set] = fr_cnt;
+        s_frlco[set] = fr_lco;
+      }
+    } else if (warp == 0) {
+      s_supc[set][lane] = sup_cnt;
+      s_supx[set][lane] = sup_carry;
+    }
+  };
+
+  // look-back, pass B and records of super-tile t, whose pass A filled set `set`
+  auto tile_back = [&](const uint32_t t, const uint32_t set) {
+    const uint32_t m = subs_in_tile(t, S, n, nsub);
+    const unsigned long long tstart = (unsigned long long)t * S;
+    uint64_t* const masks_s = masks + (size_t)set * nsub * kThreads;
+    uint32_t* const wcnt_s = s_wcnt + set * (kMaxSub * kWarps);
+    uint32_t* const wcend_s = s_wcend + set * (kMaxSub * kWarps);
+    uint32_t* const sublco_s = s_sub_lco + set * kMaxSub;
+    uint8_t* const srec_b = smem + lay.srec + set * lay.srec_set;
+    uint8_t* const wtab_b = smem + lay.wtab + set * lay.wtab_set;
+    uint8_t* const wrec_b = smem + lay.wrec + set * lay.wrec_set;
+    uint8_t* const subrec_b = smem + lay.subrec + set * lay.subrec_set;
+    const bool use_rec = MODE == kModeFree || L <= 4u;
+    const uint32_t tag = p.epoch & 0xFFFFFFu;
     // ================= look back, publish the inclusive prefix
     if (warp == 0) {
       unsigned long long K = 0;
@@ -1939,15 +1956,15 @@ __global__ void __launch_bounds__(kThreads, 3)
       unsigned long long Kin;
       uint32_t cout;
       if (MODE == kModeFree) {
-        const unsigned long long fcnt = __shfl_sync(0xffffffffu, fr_cnt, 0);
-        const long long flco = __shfl_sync(0xffffffffu, fr_lco, 0);
+        const unsigned long long fcnt = s_frcnt[set];
+        const long long flco = s_frlco[set];
         const long long sh = (long long)c - (long long)m * kTile;  // span of this super-tile
         const long long co = sh > flco ? sh : flco;
         Kin = K + fcnt;
         cout = co > 0 ? (uint32_t)co : 0u;
       } else {
-        Kin = K + __shfl_sync(0xffffffffu, sup_cnt, c);
-        cout = __shfl_sync(0xffffffffu, sup_carry, c);
+        Kin = K + s_supc[set][c];
+        cout = s_supx[set][c];
       }
       if (lane == 0) {
         if (use_rec) rec_store(p.rec, t, rec_word(tag, kStInc, Kin), rec_word(tag, kStInc, cout));
@@ -1978,15 +1995,15 @@ __global__ void __launch_bounds__(kThreads, 3)
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
       const unsigned long long gseg = sstart + sb;
-      const uint64_t mask = masks[j * kThreads + tid];
+      const uint64_t mask = masks_s[j * kThreads + tid];
       // valid input bytes of warp region `lane` (lanes 0..7 stand for the 8 warps)
       const unsigned long long wrs = sstart + (unsigned long long)lane * 2048u;
       const uint32_t wbytes = wrs >= n ? 0u : ((n - wrs) < 2048ull ? (uint32_t)(n - wrs) : 2048u);
       uint32_t x_in, cnt, wolen = 0;
       uint64_t kept;
       if (MODE == kModeFree) {
-        const uint32_t wc = lane < 8u ? s_wcnt[j * kWarps + lane] : 0u;
-        const uint32_t we = lane < 8u ? s_wcend[j * kWarps + lane] : 0u;
+        const uint32_t wc = lane < 8u ? wcnt_s[j * kWarps + lane] : 0u;
+        const uint32_t we = lane < 8u ? wcend_s[j * kWarps + lane] : 0u;
         const uint32_t pre = lanes8_excl_max(we);  // max cover end of the earlier warps
         const uint32_t covs = csub > pre ? csub : pre;
         const uint32_t wlo = lane * 2048u, whi = wlo + 2048u;
@@ -1997,7 +2014,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           // only the previous segment's last match (or the sub-tile carry) can reach here
           uint32_t cov = tid == 0 ? csub : 0u;
           if (tid > 0) {
-            const uint64_t pm = masks[j * kThreads + tid - 1];
+            const uint64_t pm = masks_s[j * kThreads + tid - 1];
             if (pm) {
               const uint32_t e = 63u - (uint32_t)__clzll((long long)pm) + L;
               if (e > 64u && e - 64u > cov) cov = e - 64u;
@@ -2020,13 +2037,13 @@ __global__ void __launch_bounds__(kThreads, 3)
         kept = mask;
         cnt = (uint32_t)__popcll(mask);
         const long long sh = (long long)csub - (long long)kTile;
-        const long long lco = (long long)s_sub_lco[j];
+        const long long lco = (long long)sublco_s[j];
         const long long nx = sh > lco ? sh : lco;
         csub = nx > 0 ? (uint32_t)nx : 0u;
       } else {
-        const uint32_t cs = (smem + lay.subrec)[j * L + cin];
-        const uint8_t* wrec = smem + lay.wrec + (size_t)j * kWarps * L;
-        const uint32_t* wt = reinterpret_cast<const uint32_t*>(smem + lay.wtab) + (size_t)j * kWarps * L;
+        const uint32_t cs = (subrec_b)[j * L + cin];
+        const uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
+        const uint32_t* wt = reinterpret_cast<const uint32_t*>(wtab_b) + (size_t)j * kWarps * L;
         uint32_t cw = 0;
         if (lane < 8u) {
           cw = wrec[lane * L + cs];
@@ -2035,7 +2052,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           wolen = wbytes - (cw < wbytes ? cw : wbytes) - wc * L + co + wc * R;
         }
         const uint32_t mycw = __shfl_sync(0xffffffffu, cw, warp);
-        x_in = (smem + lay.srec)[((size_t)j * kThreads + tid) * L + mycw];
+        x_in = (srec_b)[((size_t)j * kThreads + tid) * L + mycw];
         if (x_in >= 64u) {
           kept = 0;
           cnt = 0;
@@ -2260,7 +2277,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       O += sub_total;
       __syncthreads();
       ring.release();
-      if (tid == 0) ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
     }
 
     // ================= per-super-tile records: last kept start, totals
@@ -2287,23 +2304,84 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
       }
     }
-    // claim the next super-tile only now, when its pass A starts: a super-tile claimed
-    // early but started late would hold up the look-back of every later super-tile
-    if (tid == 0) {
-      s_q[1] = 0xFFFFFFFFu;
-      ring.shift();
-      s_fail = 0;
-      if (SEG) {
-        s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
-        if (s_q[0] != 0xFFFFFFFFu) {
-          const JobDims d = job_dims(p, S);
-          ring.issue(p, smem, lay, s_bar, s_q, S, d.n16, d.want_a, d.n, d.NT);
-        }
-      } else {
-        const uint32_t nx = atomicAdd(sched, 1u);
-        s_q[0] = nx < NT ? nx : NT;
-        ring.issue(p, smem, lay, s_bar, s_q, S, n16, want_a, n, NT);
+  };
+
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  if (tid == 0) {
+    for (int b = 0; b < kNBuf; ++b) mbar_init(&s_bar[b], 1);
+    fence_mbar_init();
+    s_fail = 0;
+    if (SEG) {
+      s_jobid = kNone;
+      s_newjob = 0;
+      s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
+      if (s_q[0] != kNone) {
+        const JobDims d = job_dims(p, S);
+        ring.push(s_q[0], 0);
+        ring.push(s_q[0], 1);
+        ring.issue(p, smem, lay, s_bar, S, d.n16, d.want_a, d.n, nsub);
       }
+    } else {
+      const uint32_t first = atomicAdd(sched, 1u);
+      s_q[0] = first < NT ? first : kNone;
+      if (s_q[0] != kNone) {
+        ring.push(s_q[0], 0);
+        ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+      }
+    }
+  }
+
+  if (SEG) {
+    // segmented launch: one super-tile at a time (the job, and its pattern, may change)
+    for (;;) {
+      __syncthreads();
+      const uint32_t t = s_q[0];
+      if (t == kNone) break;
+      if (s_newjob) {  // a super-tile of another job: its dimensions and pattern
+        setup_job();
+        __syncthreads();
+        if (tid == 0) s_newjob = 0;
+      }
+      tile_front(t, 0);
+      tile_back(t, 0);
+      // claim the next super-tile only now, when its pass A starts: a super-tile claimed
+      // early but started late would hold up the look-back of every later super-tile
+      if (tid == 0) {
+        s_fail = 0;
+        s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
+        if (s_q[0] != kNone) {
+          const JobDims d = job_dims(p, S);
+          ring.push(s_q[0], 0);
+          ring.push(s_q[0], 1);
+          ring.issue(p, smem, lay, s_bar, S, d.n16, d.want_a, d.n, nsub);
+        }
+      }
+    }
+  } else {
+    // one apply: pass A of super-tile k runs while super-tile k-1's predecessors publish
+    // their records; then k-1 looks back (its wait mostly over) and writes its output. A
+    // super-tile is still claimed when its pass A starts, so every claimed super-tile
+    // publishes its aggregate without waiting on another CTA.
+    uint32_t tprev = kNone, k = 0;
+    for (;;) {
+      __syncthreads();
+      const uint32_t tcur = s_q[0];
+      if (tcur == kNone && tprev == kNone) break;
+      if (tcur != kNone) tile_front(tcur, k & 1u);
+      if (tprev != kNone) tile_back(tprev, (k & 1u) ^ 1u);
+      if (tid == 0) {
+        uint32_t nx = kNone;
+        if (tcur != kNone) {
+          const uint32_t c = atomicAdd(sched, 1u);
+          nx = c < NT ? c : kNone;
+        }
+        s_q[0] = nx;
+        if (nx != kNone) ring.push(nx, 0);
+        if (tcur != kNone) ring.push(tcur, 1);
+        ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+      }
+      tprev = tcur;
+      ++k;
     }
   }
 
@@ -2532,11 +2610,15 @@ void prepare_pattern_fields(ReplaceParams& p, const uint8_t* pat, uint32_t L) {
 }
 
 uint32_t tile_kernel_smem_bytes(uint32_t mode, uint32_t L, uint32_t R) { return make_layout(mode, L, R).total; }
+// A single apply holds two super-tiles' tables at once (pass A of one overlaps the previous
+// one's look-back), so its super-tiles are 4 sub-tiles (64 KiB): three CTAs still fit an SM.
+constexpr uint32_t kApplySub = 4;
+
 uint32_t super_nsub(uint32_t mode, uint32_t L) {
-  if (mode == kModeFree) return kMaxSub;
+  if (mode == kModeFree) return kApplySub;
   if (mode == kModeSmall && L >= 2 && L <= 32) {
     const uint32_t by_rec = 128u / L;  // keep the per-segment carry records within 32 KiB
-    return by_rec < (uint32_t)kMaxSub ? (by_rec ? by_rec : 1u) : (uint32_t)kMaxSub;
+    return by_rec < kApplySub ? (by_rec ? by_rec : 1u) : kApplySub;
   }
   return 0;
 }
@@ -2546,7 +2628,7 @@ template <int MODE>
 cudaError_t launch_super_mode(const ReplaceParams& p, cudaStream_t st, int* grid_out) {
   static std::mutex mu;
   static unsigned long long attr_dev_mask = 0;
-  const uint32_t smem = make_layout_s(MODE, p.L, p.R, p.nsub).total;
+  const uint32_t smem = make_layout_s(MODE, p.L, p.R, p.nsub, 0u, 2u).total;  // two sets of tables
   int dev = 0;
   cudaGetDevice(&dev);
   {
