@@ -1071,10 +1071,6 @@ __device__ __forceinline__ uint64_t candidates_from_words(const uint32_t w[17], 
   return ((uint64_t)hi << 32) | lo;
 }
 
-// Output staging: a word buffer with one padding word after every 32, so threads that
-// write their (contiguous) outputs word by word land on different banks.
-__device__ __forceinline__ uint32_t stg_pad(uint32_t w) { return w + (w >> 5); }
-
 // 4 bytes at an arbitrary shared-memory byte address (two aligned loads and a funnel shift).
 __device__ __forceinline__ uint32_t ld_u32_unaligned(const uint8_t* p) {
   const uintptr_t a = reinterpret_cast<uintptr_t>(p);
@@ -1082,6 +1078,56 @@ __device__ __forceinline__ uint32_t ld_u32_unaligned(const uint8_t* p) {
   const uint32_t sh = (uint32_t)(a & 3u) * 8u;
   return sh ? __funnelshift_r(q[0], q[1], sh) : q[0];
 }
+
+// 4-bit mask of the bytes of w equal to the byte replicated in rep (bit i: byte i). Exact per
+// byte: (x & 0x7f) + 0x7f sets bit 7 of a byte iff its low 7 bits are nonzero, with no carry
+// into the next byte; the multiply gathers the four bit-7 flags into bits 28-31.
+__device__ __forceinline__ uint32_t eq_nibble(uint32_t w, uint32_t rep) {
+  const uint32_t x = w ^ rep;
+  const uint32_t nz = ((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x;
+  return ((~nz & 0x80808080u) * 0x00204081u) >> 28;
+}
+
+// 64-bit mask of the segment's bytes equal to the byte replicated in rep.
+__device__ __forceinline__ uint64_t byte_eq_mask(const uint32_t w[17], uint32_t rep) {
+  uint32_t lo = 0, hi = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    lo |= eq_nibble(w[i], rep) << (4 * i);
+    hi |= eq_nibble(w[i + 8], rep) << (4 * i);
+  }
+  return ((uint64_t)hi << 32) | lo;
+}
+
+// Candidate starts of one 64-byte segment, comparing the first min(L, 4) pattern bytes
+// (as candidates_from_words) with fewer instructions: the positions holding the first pattern
+// byte come from four bytes per operation; L = 1 needs nothing more and a doubled first byte
+// (L = 2, e.g. "aa") a shift; otherwise each such position is checked with one unaligned
+// 4-byte read, unless a lane of the warp has many of them (dense text such as a run of one
+// byte), where every window is compared.
+__device__ __forceinline__ uint64_t candidates_filtered(const uint32_t w[17], const uint8_t* seg, uint32_t p4,
+                                                        uint32_t m4, uint32_t L) {
+  const uint32_t b0 = p4 & 0xFFu;
+  const uint64_t e0 = byte_eq_mask(w, b0 * 0x01010101u);
+  if (L == 1u) return e0;
+  if (L == 2u && ((p4 >> 8) & 0xFFu) == b0) {
+    const uint64_t next = (w[16] & 0xFFu) == b0 ? 1ull : 0ull;  // byte 64: the next segment's first
+    return e0 & ((e0 >> 1) | (next << 63));
+  }
+  if (__any_sync(0xffffffffu, __popcll(e0) > 12)) return candidates_from_words(w, p4, m4);
+  uint64_t m = e0, out = 0;
+  while (m) {
+    const int b = __ffsll((long long)m) - 1;
+    m &= m - 1;
+    if (((ld_u32_unaligned(seg + b) ^ p4) & m4) == 0u) out |= 1ull << b;
+  }
+  return out;
+}
+
+// Output staging: a word buffer with one padding word after every 32, so threads that
+// write their (contiguous) outputs word by word land on different banks.
+__device__ __forceinline__ uint32_t stg_pad(uint32_t w) { return w + (w >> 5); }
+
 
 // Streams one thread's output bytes into the staging buffer: whole words are stored as
 // words; the partial first and last words (shared with the neighbouring threads) byte by
@@ -1787,7 +1833,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
       uint32_t W[17];
       load_seg_words(tb + sb, W);
-      uint64_t mask = candidates_from_words(W, p.p4, p.m4);
+      uint64_t mask = candidates_filtered(W, tb + sb, p.p4, p.m4, L);
       {
         uint32_t lo = 0, hi = 0;
         if (p.block_before > gseg) {
