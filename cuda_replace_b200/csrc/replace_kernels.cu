@@ -112,6 +112,33 @@ __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_gmem, 
       "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// L2 policies for the super-tile kernel: its input is read twice (pass A from HBM, pass B again
+// a super-tile later), so pass A's loads ask L2 to keep the lines (evict_last) and pass B's
+// loads and the output stores let them go first (evict_first).
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void bulk_load_hint(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar,
+                                               uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+          "r"(smem_u32(dst_smem)),
+      "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+// 16-byte output store that L2 may evict first (the output is not read again by this kernel).
+__device__ __forceinline__ void st_out16(uint8_t* dst, const uint4& v) {
+  asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.u32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(dst), "r"(v.x),
+               "r"(v.y), "r"(v.z), "r"(v.w), "l"(l2_policy_evict_first())
+               : "memory");
+}
 __device__ __forceinline__ void bulk_store(void* dst_gmem, const void* src_smem, uint32_t bytes) {
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem),
                "r"(smem_u32(src_smem)), "r"(bytes)
@@ -1642,7 +1669,8 @@ struct LoadRing {
       const uint32_t b = issued % kNBuf;
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&bars[b], bytes);
-      bulk_load(smem + lay.in0 + b * lay.inbytes, p.in + start, bytes, &bars[b]);
+      bulk_load_hint(smem + lay.in0 + b * lay.inbytes, p.in + start, bytes, &bars[b],
+                     ph_k0 == 0 ? l2_policy_evict_last() : l2_policy_evict_first());
       ++issued;
       if (++ij == m) {
         ij = 0;
@@ -2160,7 +2188,7 @@ __global__ void __launch_bounds__(kThreads, 3)
             const uint32_t a = off0 - r + ((c - c0) << 4);
             const uint4 A = *reinterpret_cast<const uint4*>(tb + a);
             const uint4 B = *reinterpret_cast<const uint4*>(tb + a + 16u);
-            *reinterpret_cast<uint4*>(p.out + ga + ((unsigned long long)c << 4)) = extract16(A, B, q, sh);
+            st_out16(p.out + ga + ((unsigned long long)c << 4), extract16(A, B, q, sh));
           }
           unsigned long long b;
           bool ok;
@@ -2178,7 +2206,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           uint32_t c = c0 + lane;
           uint32_t ph = (uint32_t)((ga + ((unsigned long long)c << 4) - g0) % R);
           for (; c < c1; c += 32u) {
-            *reinterpret_cast<uint4*>(p.out + ga + ((unsigned long long)c << 4)) = t16[ph];
+            st_out16(p.out + ga + ((unsigned long long)c << 4), t16[ph]);
             ph += step512;
             if (ph >= R) ph -= R;
           }
@@ -2256,7 +2284,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           v.y = stg[stg_pad(w + 1)];
           v.z = stg[stg_pad(w + 2)];
           v.w = stg[stg_pad(w + 3)];
-          *reinterpret_cast<uint4*>(p.out + ga + ((unsigned long long)c << 4)) = v;
+          st_out16(p.out + ga + ((unsigned long long)c << 4), v);
         }
         {
           // head bytes [g0, ga + 16*c0) on lanes 0-15, tail bytes [ga + 16*c1, gend) on 16-31;
