@@ -986,6 +986,7 @@ struct LayoutS {
   uint32_t masks_set, srec_set, wtab_set, wrec_set, subrec_set;  // bytes of one set of per-super-tile tables
   uint32_t rs, inbytes;
   uint32_t wstage_words;  // padded staging words per warp (its 2 KiB of input may grow 3x)
+  uint32_t wstage_cap;    // bytes one warp can stage (before the padding words)
 };
 
 // Output bytes one 16 KiB sub-tile can produce, capped at three times its input.
@@ -1008,6 +1009,7 @@ __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_
   {
     const uint32_t words = (2048u * (ratio ? ratio : stage_ratio(L, R)) + 48u) / 4u;
     s.wstage_words = words + words / 32u + 2u;
+    s.wstage_cap = words * 4u;
   }
   s.outb = off;
   off += align_up_u32(kWarps * s.wstage_words * 4u, 16);
@@ -1693,6 +1695,7 @@ struct LoadRing {
     }
     return smem + lay.in0 + b * lay.inbytes;
   }
+  // After a block barrier: every thread is done with the current buffer.
   __device__ __forceinline__ void release() { ++consumed; }
 };
 
@@ -1803,7 +1806,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   // the job's dimensions and pattern: once (one apply) or whenever the job changes (segmented)
   uint32_t L = 0, R = 0, NT = 0, carry0 = 0, want_a = 0, step4 = 0, step512 = 0;
   unsigned long long n_all = 0, n = 0, n16 = 0;
-  bool warp_stage = false, rep_table = false;
+  bool rep_table = false;
   auto setup_job = [&]() {
     const JobDims d = job_dims(p, S);
     n_all = d.n_all;
@@ -1814,7 +1817,6 @@ __global__ void __launch_bounds__(kThreads, 3)
     want_a = d.want_a;
     L = p.L;
     R = p.R;
-    warp_stage = R <= 3u * L;  // every warp's output fits its staging area
     rep_table = R >= 1u && R <= 64u;
     step4 = R ? 4u % R : 0u;
     step512 = R ? 512u % R : 0u;
@@ -2167,6 +2169,16 @@ __global__ void __launch_bounds__(kThreads, 3)
       sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
 
       const bool fits = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
+      // every warp's output of this sub-tile fits its staging area (with the up to 15 bytes of
+      // alignment in front): the warp paths; otherwise the whole block writes windows. Lanes
+      // 0-7 of every warp hold the eight lengths, so the choice is the same in every warp.
+      uint32_t wmax = lane < 8u ? wolen : 0u;
+#pragma unroll
+      for (int d = 4; d >= 1; d >>= 1) {
+        const uint32_t o = __shfl_xor_sync(0xffffffffu, wmax, d);
+        wmax = o > wmax ? o : wmax;
+      }
+      const bool warp_stage = __shfl_sync(0xffffffffu, wmax, 0) + 15u <= lay.wstage_cap;
       if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
       // warp output mode: no kept match in the warp (a copy of its input), or no literal byte
       // (a run of replacements), or mixed
@@ -2304,7 +2316,9 @@ __global__ void __launch_bounds__(kThreads, 3)
           }
         }
       } else if (fits && !failed) {
-        // very large expansions: windows of the sub-tile output, byte by byte
+        // very large expansions: windows of the sub-tile output, byte by byte (the windows
+        // share the staging area with the warps' own staging, which the block barrier at the
+        // end of every sub-tile keeps apart)
         const uint32_t ooff = wbase + toff;
         const uint32_t sub_olen = sub_total;
         for (uint32_t w0 = 0; w0 < sub_olen; w0 += kOutWin) {

@@ -278,3 +278,24 @@ def test_native_stream_limits_and_mixed_pairs(cr_lib):
     src = (b"ab" * 30000 + b"c") * 3
     pairs = [(b"c", b"cc"), (b"ab" * 20, b"Z"), (b"", b"-"), (b"-Z", b"z"), (b"b-", b"")]
     assert Wr.gpu_replace_streaming(cr_lib, src, pairs, chunk_bytes=10000) == chain(src, pairs)
+
+
+@pytest.mark.parametrize("L,R", [(40, 40), (100, 100), (33, 64), (2048, 2048), (3000, 900), (200, 600)])
+def test_matches_overhanging_warp_regions(cr_lib, L, R):
+    """A match that starts near the end of a 2 KiB warp region and runs past it makes that
+    region's output up to 2047 + R bytes: more than the input it covers. Plant such matches
+    at every region end (and inside) and compare with bytes.replace."""
+    rng = random.Random(L * 7 + R)
+    pat = bytes(rng.randrange(1, 256) for _ in range(L))
+    rep = bytes(rng.randrange(256) for _ in range(R))
+    n = 40 * 2048 + 123
+    src = bytearray(rng.randrange(256) for _ in range(n))
+    pos = 2047
+    while pos + L <= n:
+        src[pos:pos + L] = pat
+        pos += max(L + rng.randrange(0, 64), 2048 * (1 + L // 2048))
+    for pos in range(5, n - L, 8192 + 1000):
+        if all(src[pos + k] != 0x00 for k in range(1)):
+            src[pos:pos + L] = pat
+    src = bytes(src)
+    assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep)
