@@ -1543,6 +1543,24 @@ template <int LL>
 __device__ __forceinline__ void ks_warp_tables(uint64_t mask, uint32_t inv_l, uint64_t stride, uint8_t* srec_row,
                                                uint32_t* wtab_row) {
   const uint32_t lane = threadIdx.x & 31u;
+  if (__all_sync(0xffffffffu, mask == ~0ull)) {
+    // every position of the warp's 2 KiB is a candidate (a run such as "aaaa" for "aa"): from
+    // carry-in c the greedy keeps c, c + L, c + 2L, ... so both tables have a closed form
+    const uint32_t off = 64u * lane;
+#pragma unroll
+    for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
+      const uint32_t q = off > c ? (off - c + LL - 1u) / LL : 0u;  // kept starts before this segment
+      srec_row[c] = (uint8_t)(c + q * LL - off);
+    }
+    if (lane == 31) {
+#pragma unroll
+      for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
+        const uint32_t cnt = (2048u - c + LL - 1u) / LL;
+        wtab_row[c] = cnt | ((c + cnt * LL - 2048u) << 16);
+      }
+    }
+    return;
+  }
   uint32_t ent[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
   for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
