@@ -1882,13 +1882,15 @@ __global__ void __launch_bounds__(kThreads, 3)
       uint32_t W[17];
       load_seg_words(tb + sb, W);
       uint64_t mask = candidates_filtered(W, tb + sb, p.p4, p.m4, L);
-      {
+      // bounds: candidates p in [block_before, lim); a sub-tile inside both needs no masking
+      const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
+      const unsigned long long sub0 = tstart + (unsigned long long)j * kTile;
+      if (sub0 < p.block_before || sub0 + kTile > lim) {
         uint32_t lo = 0, hi = 0;
         if (p.block_before > gseg) {
           const unsigned long long d = p.block_before - gseg;
           lo = d < 64ull ? (uint32_t)d : 64u;
         }
-        const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
         if (lim > gseg) {
           const unsigned long long d = lim - gseg;
           hi = d < 64ull ? (uint32_t)d : 64u;
@@ -1899,14 +1901,9 @@ __global__ void __launch_bounds__(kThreads, 3)
       masks_s[j * kThreads + tid] = mask;
       if (MODE == kModeFree) {
         // every candidate is kept: per warp, the count and how far its last match reaches
-        uint32_t cnt = (uint32_t)__popcll(mask);
-        uint32_t cend = mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u;
-#pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {
-          cnt += __shfl_xor_sync(0xffffffffu, cnt, d);
-          const uint32_t o = __shfl_xor_sync(0xffffffffu, cend, d);
-          cend = o > cend ? o : cend;
-        }
+        const uint32_t cnt = __reduce_add_sync(0xffffffffu, (uint32_t)__popcll(mask));
+        const uint32_t cend = __reduce_max_sync(
+            0xffffffffu, mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u);
         if (lane == 0) {
           wcnt_s[j * kWarps + warp] = cnt;
           wcend_s[j * kWarps + warp] = cend;
@@ -2190,13 +2187,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       // every warp's output of this sub-tile fits its staging area (with the up to 15 bytes of
       // alignment in front): the warp paths; otherwise the whole block writes windows. Lanes
       // 0-7 of every warp hold the eight lengths, so the choice is the same in every warp.
-      uint32_t wmax = lane < 8u ? wolen : 0u;
-#pragma unroll
-      for (int d = 4; d >= 1; d >>= 1) {
-        const uint32_t o = __shfl_xor_sync(0xffffffffu, wmax, d);
-        wmax = o > wmax ? o : wmax;
-      }
-      const bool warp_stage = __shfl_sync(0xffffffffu, wmax, 0) + 15u <= lay.wstage_cap;
+      const bool warp_stage = __reduce_max_sync(0xffffffffu, lane < 8u ? wolen : 0u) + 15u <= lay.wstage_cap;
       if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
       // warp output mode: no kept match in the warp (a copy of its input), or no literal byte
       // (a run of replacements), or mixed
