@@ -1717,6 +1717,65 @@ struct LoadRing {
   __device__ __forceinline__ void release() { ++consumed; }
 };
 
+// One warp's output when it is a copy of its input: wtot bytes from tile byte srcw, written at
+// out[g0, g0 + wtot) with aligned 16-byte stores (funnel-shifted from shared memory); the
+// partial 16-byte chunks at both ends one byte per lane (the neighbouring regions own their
+// other bytes).
+__device__ __forceinline__ void warp_emit_literal(uint8_t* out, const uint8_t* tb, unsigned long long g0,
+                                                  uint32_t wtot, uint32_t srcw) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long ga = g0 & ~15ull;
+  const unsigned long long gend = g0 + wtot;
+  const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);  // first whole 16-byte chunk
+  const uint32_t c1 = (uint32_t)((gend - ga) >> 4);        // end of the whole chunks
+  const uint32_t off0 = srcw + (uint32_t)(ga + ((unsigned long long)c0 << 4) - g0);
+  const uint32_t r = off0 & 15u, q = r >> 2, sh = (r & 3u) * 8u;
+  for (uint32_t c = c0 + lane; c < c1; c += 32u) {
+    const uint32_t a = off0 - r + ((c - c0) << 4);
+    const uint4 A = *reinterpret_cast<const uint4*>(tb + a);
+    const uint4 B = *reinterpret_cast<const uint4*>(tb + a + 16u);
+    st_out16(out + ga + ((unsigned long long)c << 4), extract16(A, B, q, sh));
+  }
+  unsigned long long b;
+  bool ok;
+  if (c0 < c1) {
+    b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
+    ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
+  } else {
+    b = g0 + lane;
+    ok = b < gend;
+  }
+  if (ok) out[b] = tb[srcw + (uint32_t)(b - g0)];
+}
+
+// One warp's output when it is a run of replacements: 16 bytes per phase from the table t16
+// (the replacement repeated from every phase), the partial chunks from rs byte by byte.
+__device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16, const uint8_t* rs, uint32_t R,
+                                                  uint32_t step512, unsigned long long g0, uint32_t wtot) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long ga = g0 & ~15ull;
+  const unsigned long long gend = g0 + wtot;
+  const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);
+  const uint32_t c1 = (uint32_t)((gend - ga) >> 4);
+  uint32_t c = c0 + lane;
+  uint32_t ph = (uint32_t)((ga + ((unsigned long long)c << 4) - g0) % R);
+  for (; c < c1; c += 32u) {
+    st_out16(out + ga + ((unsigned long long)c << 4), t16[ph]);
+    ph += step512;
+    if (ph >= R) ph -= R;
+  }
+  unsigned long long b;
+  bool ok;
+  if (c0 < c1) {
+    b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
+    ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
+  } else {
+    b = g0 + lane;
+    ok = b < gend;
+  }
+  if (ok) out[b] = rs[(uint32_t)((b - g0) % R)];
+}
+
 // Input length, output range and super-tile count of the job described by p.
 struct JobDims {
   unsigned long long n_all, n, n16;
@@ -2090,8 +2149,9 @@ __global__ void __launch_bounds__(kThreads, 3)
       // valid input bytes of warp region `lane` (lanes 0..7 stand for the 8 warps)
       const unsigned long long wrs = sstart + (unsigned long long)lane * 2048u;
       const uint32_t wbytes = wrs >= n ? 0u : ((n - wrs) < 2048ull ? (uint32_t)(n - wrs) : 2048u);
-      uint32_t x_in, cnt, wolen = 0;
+      uint32_t x_in = 0, cnt, wolen = 0;
       uint64_t kept;
+      uint32_t csub_in = 0, covs_l = 0, ewc = 0, ewcov = 0;  // kModeFree: kept for x_in and the warp paths
       if (MODE == kModeFree) {
         const uint32_t wc = lane < 8u ? wcnt_s[j * kWarps + lane] : 0u;
         const uint32_t we = lane < 8u ? wcend_s[j * kWarps + lane] : 0u;
@@ -2101,30 +2161,10 @@ __global__ void __launch_bounds__(kThreads, 3)
         const uint32_t wcov = covs > wlo ? covs - wlo : 0u;
         const uint32_t over = we > whi ? we - whi : 0u;
         wolen = wbytes - (wcov < wbytes ? wcov : wbytes) - wc * L + over + wc * R;
-        if (L <= 64u) {
-          // only the previous segment's last match (or the sub-tile carry) can reach here
-          uint32_t cov = tid == 0 ? csub : 0u;
-          if (tid > 0) {
-            const uint64_t pm = masks_s[j * kThreads + tid - 1];
-            if (pm) {
-              const uint32_t e = 63u - (uint32_t)__clzll((long long)pm) + L;
-              if (e > 64u && e - 64u > cov) cov = e - 64u;
-            }
-          }
-          x_in = cov;
-        } else {
-          uint32_t ce = mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u;
-#pragma unroll
-          for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t o = __shfl_up_sync(0xffffffffu, ce, d);
-            if (lane >= (uint32_t)d) ce = o > ce ? o : ce;
-          }
-          uint32_t prev = __shfl_up_sync(0xffffffffu, ce, 1);
-          if (lane == 0) prev = 0;
-          const uint32_t pw = __shfl_sync(0xffffffffu, covs, warp);
-          const uint32_t cv = prev > pw ? prev : pw;
-          x_in = cv > sb ? cv - sb : 0u;
-        }
+        csub_in = csub;
+        covs_l = covs;
+        ewc = wc;
+        ewcov = wcov < wbytes ? wcov : wbytes;
         kept = mask;
         cnt = (uint32_t)__popcll(mask);
         const long long sh = (long long)csub - (long long)kTile;
@@ -2153,6 +2193,61 @@ __global__ void __launch_bounds__(kThreads, 3)
           cnt = w.cnt;
         }
       }
+      // ---- free mode, L <= 64: a warp whose output is a copy of its input or a run of
+      // replacements is written straight from the pass-A tables, with no per-thread scan
+      uint32_t wbase = 0, sub_total = 0;
+      bool done = false;
+      if (MODE == kModeFree && L <= 64u) {
+        const uint32_t cut0 = __ballot_sync(0xffffffffu, lane < 8u && wbytes != 0u && wbytes < 2048u);
+        if (!cut0) {
+          lanes8_sum(wolen, &wbase, &sub_total);
+          wbase = __shfl_sync(0xffffffffu, wbase, warp);
+          sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
+          const bool fits0 = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
+          const bool stage0 =
+              __reduce_max_sync(0xffffffffu, lane < 8u ? wolen : 0u) + 15u <= lay.wstage_cap;
+          const uint32_t wcw = __shfl_sync(0xffffffffu, ewc, warp);
+          const uint32_t wlw = __shfl_sync(0xffffffffu, wolen, warp);
+          if (fits0 && !failed && stage0 && (wcw == 0u || (rep_table && wlw == wcw * R))) {
+            done = true;  // the same in every lane of the warp
+            if (wlw) {
+              if (wcw == 0u)
+                warp_emit_literal(p.out, tb, O + wbase, wlw, warp * 2048u + __shfl_sync(0xffffffffu, ewcov, warp));
+              else
+                warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512,
+                                  O + wbase, wlw);
+            }
+            if (mask) last_abs = (long long)(gseg + (63u - (uint32_t)__clzll((long long)mask)));
+          }
+        }
+      }
+      if (!done) {
+      if (MODE == kModeFree) {
+        if (L <= 64u) {
+          // only the previous segment's last match (or the sub-tile carry) can reach here
+          uint32_t cov = tid == 0 ? csub_in : 0u;
+          if (tid > 0) {
+            const uint64_t pm = masks_s[j * kThreads + tid - 1];
+            if (pm) {
+              const uint32_t e = 63u - (uint32_t)__clzll((long long)pm) + L;
+              if (e > 64u && e - 64u > cov) cov = e - 64u;
+            }
+          }
+          x_in = cov;
+        } else {
+          uint32_t ce = mask ? sb + (63u - (uint32_t)__clzll((long long)mask)) + L : 0u;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, ce, d);
+            if (lane >= (uint32_t)d) ce = o > ce ? o : ce;
+          }
+          uint32_t prev = __shfl_up_sync(0xffffffffu, ce, 1);
+          if (lane == 0) prev = 0;
+          const uint32_t pw = __shfl_sync(0xffffffffu, covs_l, warp);
+          const uint32_t cv = prev > pw ? prev : pw;
+          x_in = cv > sb ? cv - sb : 0u;
+        }
+      }
       const uint32_t V = gseg >= n ? 0u : ((n - gseg) < 64ull ? (uint32_t)(n - gseg) : 64u);
       uint32_t covered = x_in < V ? x_in : V;
       if (cnt) {
@@ -2178,7 +2273,6 @@ __global__ void __launch_bounds__(kThreads, 3)
         __syncthreads();
         if (lane == cw) wolen = s_cutlen;
       }
-      uint32_t wbase, sub_total;
       lanes8_sum(wolen, &wbase, &sub_total);
       wbase = __shfl_sync(0xffffffffu, wbase, warp);
       sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
@@ -2194,53 +2288,13 @@ __global__ void __launch_bounds__(kThreads, 3)
       const uint32_t notlit = __ballot_sync(0xffffffffu, cnt != 0u || (lane > 0u && x_in != 0u));
       const uint32_t notrep = __ballot_sync(0xffffffffu, olen != cnt * R);
       if (fits && !failed && warp_stage && wtot != 0u && (notlit == 0u || (notrep == 0u && rep_table))) {
-        const unsigned long long g0 = O + wbase;
-        const unsigned long long ga = g0 & ~15ull;
-        const unsigned long long gend = g0 + wtot;
-        const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);  // first whole 16-byte chunk
-        const uint32_t c1 = (uint32_t)((gend - ga) >> 4);        // end of the whole chunks
         if (notlit == 0u) {
-          // ---- LITERAL: output = input bytes [warp start + x0, ...): aligned 16-byte copies
-          const uint32_t x0 = __shfl_sync(0xffffffffu, x_in, 0);
-          const uint32_t srcw = warp * 2048u + x0;  // tile byte of the region's first output byte
-          const uint32_t off0 = srcw + (uint32_t)(ga + ((unsigned long long)c0 << 4) - g0);
-          const uint32_t r = off0 & 15u, q = r >> 2, sh = (r & 3u) * 8u;
-          for (uint32_t c = c0 + lane; c < c1; c += 32u) {
-            const uint32_t a = off0 - r + ((c - c0) << 4);
-            const uint4 A = *reinterpret_cast<const uint4*>(tb + a);
-            const uint4 B = *reinterpret_cast<const uint4*>(tb + a + 16u);
-            st_out16(p.out + ga + ((unsigned long long)c << 4), extract16(A, B, q, sh));
-          }
-          unsigned long long b;
-          bool ok;
-          if (c0 < c1) {
-            b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
-            ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
-          } else {
-            b = g0 + lane;
-            ok = b < gend;
-          }
-          if (ok) p.out[b] = tb[srcw + (uint32_t)(b - g0)];
+          // ---- LITERAL: output = input bytes [warp start + x0, ...)
+          warp_emit_literal(p.out, tb, O + wbase, wtot, warp * 2048u + __shfl_sync(0xffffffffu, x_in, 0));
         } else {
-          // ---- REPLACE: output = the replacement repeated, 16 bytes per phase from a table
-          const uint4* t16 = reinterpret_cast<const uint4*>(smem + lay.tab16);
-          uint32_t c = c0 + lane;
-          uint32_t ph = (uint32_t)((ga + ((unsigned long long)c << 4) - g0) % R);
-          for (; c < c1; c += 32u) {
-            st_out16(p.out + ga + ((unsigned long long)c << 4), t16[ph]);
-            ph += step512;
-            if (ph >= R) ph -= R;
-          }
-          unsigned long long b;
-          bool ok;
-          if (c0 < c1) {
-            b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
-            ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
-          } else {
-            b = g0 + lane;
-            ok = b < gend;
-          }
-          if (ok) p.out[b] = rs[(uint32_t)((b - g0) % R)];
+          // ---- REPLACE: output = the replacement repeated
+          warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, O + wbase,
+                            wtot);
         }
       } else if (fits && !failed && warp_stage) {
         uint32_t W[17];
@@ -2371,6 +2425,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           __syncthreads();
         }
       }
+      }  // !done
       O += sub_total;
       __syncthreads();
       ring.release();
