@@ -2181,23 +2181,18 @@ __global__ void __launch_bounds__(kThreads, 3)
           const uint32_t e = wt[lane * L + cw];
           const uint32_t wc = e & 0xFFFFu, co = e >> 16;
           wolen = wbytes - (cw < wbytes ? cw : wbytes) - wc * L + co + wc * R;
+          ewc = wc;
+          ewcov = cw < wbytes ? cw : wbytes;
         }
-        const uint32_t mycw = __shfl_sync(0xffffffffu, cw, warp);
-        x_in = (srec_b)[((size_t)j * kThreads + tid) * L + mycw];
-        if (x_in >= 64u) {
-          kept = 0;
-          cnt = 0;
-        } else {
-          const Walk w = seg_walk(mask, x_in, L, p.inv_l, p.stride_mask);
-          kept = w.kept;
-          cnt = w.cnt;
-        }
+        covs_l = cw;  // kModeSmall: the carry into each warp region (lanes 0-7)
+        kept = 0;
+        cnt = 0;
       }
-      // ---- free mode, L <= 64: a warp whose output is a copy of its input or a run of
-      // replacements is written straight from the pass-A tables, with no per-thread scan
+      // ---- L <= 64: a warp whose output is a copy of its input or a run of replacements is
+      // written straight from the pass-A tables, with no per-thread walk or scan
       uint32_t wbase = 0, sub_total = 0;
       bool done = false;
-      if (MODE == kModeFree && L <= 64u) {
+      if (L <= 64u) {
         const uint32_t cut0 = __ballot_sync(0xffffffffu, lane < 8u && wbytes != 0u && wbytes < 2048u);
         if (!cut0) {
           lanes8_sum(wolen, &wbase, &sub_total);
@@ -2208,16 +2203,24 @@ __global__ void __launch_bounds__(kThreads, 3)
               __reduce_max_sync(0xffffffffu, lane < 8u ? wolen : 0u) + 15u <= lay.wstage_cap;
           const uint32_t wcw = __shfl_sync(0xffffffffu, ewc, warp);
           const uint32_t wlw = __shfl_sync(0xffffffffu, wolen, warp);
-          if (fits0 && !failed && stage0 && (wcw == 0u || (rep_table && wlw == wcw * R))) {
+          const uint32_t x0w = __shfl_sync(0xffffffffu, ewcov, warp);  // bytes covered at the region start
+          // copy only (no kept start), nothing to write (all covered, R = 0), or replacements only
+          if (fits0 && !failed && stage0 && (wcw == 0u || wlw == 0u || (rep_table && wlw == wcw * R))) {
             done = true;  // the same in every lane of the warp
             if (wlw) {
               if (wcw == 0u)
-                warp_emit_literal(p.out, tb, O + wbase, wlw, warp * 2048u + __shfl_sync(0xffffffffu, ewcov, warp));
+                warp_emit_literal(p.out, tb, O + wbase, wlw, warp * 2048u + x0w);
               else
                 warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512,
                                   O + wbase, wlw);
             }
-            if (mask) last_abs = (long long)(gseg + (63u - (uint32_t)__clzll((long long)mask)));
+            if (MODE == kModeFree) {
+              if (mask) last_abs = (long long)(gseg + (63u - (uint32_t)__clzll((long long)mask)));
+            } else if (wcw != 0u && lane == 0) {
+              // a region with no literal byte: its kept starts are cw, cw + L, ... (the block
+              // maximum over threads of the last kept start needs only the warp's last one)
+              last_abs = (long long)(sstart + warp * 2048u + x0w + (unsigned long long)(wcw - 1u) * L);
+            }
           }
         }
       }
@@ -2246,6 +2249,14 @@ __global__ void __launch_bounds__(kThreads, 3)
           const uint32_t pw = __shfl_sync(0xffffffffu, covs_l, warp);
           const uint32_t cv = prev > pw ? prev : pw;
           x_in = cv > sb ? cv - sb : 0u;
+        }
+      } else {
+        const uint32_t mycw = __shfl_sync(0xffffffffu, covs_l, warp);
+        x_in = (srec_b)[((size_t)j * kThreads + tid) * L + mycw];
+        if (x_in < 64u) {
+          const Walk w = seg_walk(mask, x_in, L, p.inv_l, p.stride_mask);
+          kept = w.kept;
+          cnt = w.cnt;
         }
       }
       const uint32_t V = gseg >= n ? 0u : ((n - gseg) < 64ull ? (uint32_t)(n - gseg) : 64u);
