@@ -1153,6 +1153,50 @@ __device__ __forceinline__ uint64_t candidates_filtered(const uint32_t w[17], co
   return out;
 }
 
+// candidates_filtered for the 64-byte segment at seg (shared memory), reading it without bank
+// conflicts: lanes 64 bytes apart would hit the same banks four at a time, so each pair of
+// lanes starts at another of its four 16-byte chunks; the first-byte mask is built in that
+// rotated order and rotated back (a 64-bit rotate). Only the rare dense branch reads the
+// segment in order.
+__device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t p4, uint32_t m4, uint32_t L) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t rot = (lane >> 1) & 3u;
+  const uint4* v = reinterpret_cast<const uint4*>(seg);
+  const uint4 q0 = v[rot], q1 = v[(rot + 1u) & 3u], q2 = v[(rot + 2u) & 3u], q3 = v[(rot + 3u) & 3u];
+  const uint32_t b0 = p4 & 0xFFu, rep = b0 * 0x01010101u;
+  const uint32_t lo = eq_nibble(q0.x, rep) | (eq_nibble(q0.y, rep) << 4) | (eq_nibble(q0.z, rep) << 8) |
+                      (eq_nibble(q0.w, rep) << 12) | (eq_nibble(q1.x, rep) << 16) | (eq_nibble(q1.y, rep) << 20) |
+                      (eq_nibble(q1.z, rep) << 24) | (eq_nibble(q1.w, rep) << 28);
+  const uint32_t hi = eq_nibble(q2.x, rep) | (eq_nibble(q2.y, rep) << 4) | (eq_nibble(q2.z, rep) << 8) |
+                      (eq_nibble(q2.w, rep) << 12) | (eq_nibble(q3.x, rep) << 16) | (eq_nibble(q3.y, rep) << 20) |
+                      (eq_nibble(q3.z, rep) << 24) | (eq_nibble(q3.w, rep) << 28);
+  const uint64_t er = ((uint64_t)hi << 32) | lo;  // chunk (rot + k) & 3 at bits 16k
+  const uint32_t sh = 16u * rot;
+  const uint64_t e0 = sh ? ((er << sh) | (er >> (64u - sh))) : er;
+  if (L == 1u) return e0;
+  if (L == 2u && ((p4 >> 8) & 0xFFu) == b0) {
+    // byte 64: the next lane's first word (chunk 0 of the next segment), from shared memory
+    // for the last lane
+    const uint32_t nat0 = rot == 0u ? q0.x : (rot == 1u ? q3.x : (rot == 2u ? q2.x : q1.x));
+    uint32_t w64 = __shfl_down_sync(0xffffffffu, nat0, 1);
+    if (lane == 31u) w64 = *reinterpret_cast<const uint32_t*>(seg + 64);
+    const uint64_t next = (w64 & 0xFFu) == b0 ? 1ull : 0ull;
+    return e0 & ((e0 >> 1) | (next << 63));
+  }
+  if (__any_sync(0xffffffffu, __popcll(e0) > 12)) {
+    uint32_t w[17];
+    load_seg_words(seg, w);
+    return candidates_from_words(w, p4, m4);
+  }
+  uint64_t m = e0, out = 0;
+  while (m) {
+    const int b = __ffsll((long long)m) - 1;
+    m &= m - 1;
+    if (((ld_u32_unaligned(seg + b) ^ p4) & m4) == 0u) out |= 1ull << b;
+  }
+  return out;
+}
+
 // Output staging: a word buffer with one padding word after every 32, so threads that
 // write their (contiguous) outputs word by word land on different banks.
 __device__ __forceinline__ uint32_t stg_pad(uint32_t w) { return w + (w >> 5); }
@@ -1938,9 +1982,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
-      uint32_t W[17];
-      load_seg_words(tb + sb, W);
-      uint64_t mask = candidates_filtered(W, tb + sb, p.p4, p.m4, L);
+      uint64_t mask = candidates_seg(tb + sb, p.p4, p.m4, L);
       // bounds: candidates p in [block_before, lim); a sub-tile inside both needs no masking
       const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
       const unsigned long long sub0 = tstart + (unsigned long long)j * kTile;
