@@ -2045,13 +2045,14 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
 
     // ================= fold the sub-tiles into the super-tile function
+    // (warp 1, so that warp 0 can start the previous super-tile's look-back at the same time)
     const bool use_rec = MODE == kModeFree || L <= 4u;
     const uint32_t tag = p.epoch & 0xFFFFFFu;
-    unsigned long long fr_cnt = 0;  // kModeFree: thread 0
+    unsigned long long fr_cnt = 0;  // kModeFree: lane 0 of warp 1
     long long fr_lco = 0;
-    uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 0, lane = carry-in
+    uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 1, lane = carry-in
     if (MODE == kModeFree) {
-      if (tid == 0) {
+      if (tid == 32u) {
         for (uint32_t j = 0; j < m; ++j) {
           uint32_t tot_cnt = 0, tot_cend = 0;
           for (int w = 0; w < kWarps; ++w) {
@@ -2068,7 +2069,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         if (t > 0)
           rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
       }
-    } else if (warp == 0) {
+    } else if (warp == 1) {
       const uint32_t* wt = reinterpret_cast<const uint32_t*>(wtab_b);
       for (uint32_t j = 0; j < m; ++j) {
         uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
@@ -2103,11 +2104,11 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
 
     if (MODE == kModeFree) {
-      if (tid == 0) {
+      if (tid == 32u) {
         s_frcnt[set] = fr_cnt;
         s_frlco[set] = fr_lco;
       }
-    } else if (warp == 0) {
+    } else if (warp == 1) {
       s_supc[set][lane] = sup_cnt;
       s_supx[set][lane] = sup_carry;
     }
@@ -2548,6 +2549,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         if (tid == 0) s_newjob = 0;
       }
       tile_front(t, 0);
+      __syncthreads();  // the fold (warp 1) is done before this super-tile's look-back (warp 0)
       tile_back(t, 0);
       // claim the next super-tile only now, when its pass A starts: a super-tile claimed
       // early but started late would hold up the look-back of every later super-tile
