@@ -1699,25 +1699,21 @@ __device__ __forceinline__ uint32_t subs_in_tile(uint32_t tile, unsigned long lo
 // `consumed` count; only thread 0 issues (and tracks the issue position).
 struct LoadRing {
   uint32_t issued, consumed;
-  uint32_t ij;                          // next sub-tile of the head phase
-  uint32_t nph;                         // phases queued (at most 2)
-  uint32_t ph_t0, ph_k0, ph_t1, ph_k1;  // queued phases: super-tile, kind (0: pass A, 1: pass B)
+  uint32_t ij;   // next sub-tile of the head phase
+  uint32_t qh;   // head of the phase queue
+  uint32_t nph;  // phases queued (at most kPhases)
+  uint32_t* q;   // the queue in shared memory: super-tile << 1 | kind (0: pass A, 1: pass B)
+  static constexpr uint32_t kPhases = 4;
 
-  __device__ __forceinline__ void init() {
+  __device__ __forceinline__ void init(uint32_t* qs) {
     issued = consumed = 0;
-    ij = nph = 0;
-    ph_t0 = ph_k0 = ph_t1 = ph_k1 = 0;
+    ij = qh = nph = 0;
+    q = qs;
   }
   // Thread 0: queue the loads of one pass over super-tile t (kind 0: sub-tiles with their
   // halo, for pass A; kind 1: sub-tiles, for pass B), consumed in the order queued.
   __device__ __forceinline__ void push(uint32_t t, uint32_t kind) {
-    if (nph == 0) {
-      ph_t0 = t;
-      ph_k0 = kind;
-    } else {
-      ph_t1 = t;
-      ph_k1 = kind;
-    }
+    q[(qh + nph) & (kPhases - 1u)] = (t << 1) | kind;
     ++nph;
   }
   // Thread 0: keep up to kNBuf loads in flight.
@@ -1725,21 +1721,22 @@ struct LoadRing {
                                         unsigned long long S, unsigned long long n16, uint32_t want_a,
                                         unsigned long long n, uint32_t nsub) {
     while (issued - consumed < (uint32_t)kNBuf && nph > 0) {
-      const uint32_t m = subs_in_tile(ph_t0, S, n, nsub);
-      const unsigned long long start = (unsigned long long)ph_t0 * S + (unsigned long long)ij * kTile;
+      const uint32_t e = q[qh];
+      const uint32_t t = e >> 1, kind = e & 1u;
+      const uint32_t m = subs_in_tile(t, S, n, nsub);
+      const unsigned long long start = (unsigned long long)t * S + (unsigned long long)ij * kTile;
       const unsigned long long avail = n16 - start;
-      const uint32_t want = ph_k0 == 0 ? want_a : (uint32_t)kTile;
+      const uint32_t want = kind == 0 ? want_a : (uint32_t)kTile;
       const uint32_t bytes = avail < want ? (uint32_t)avail : want;
       const uint32_t b = issued % kNBuf;
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&bars[b], bytes);
       bulk_load_hint(smem + lay.in0 + b * lay.inbytes, p.in + start, bytes, &bars[b],
-                     ph_k0 == 0 ? l2_policy_evict_last() : l2_policy_evict_first());
+                     kind == 0 ? l2_policy_evict_last() : l2_policy_evict_first());
       ++issued;
       if (++ij == m) {
         ij = 0;
-        ph_t0 = ph_t1;
-        ph_k0 = ph_k1;
+        qh = (qh + 1u) & (kPhases - 1u);
         --nph;
       }
     }
@@ -1802,7 +1799,8 @@ __device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16
   const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);
   const uint32_t c1 = (uint32_t)((gend - ga) >> 4);
   uint32_t c = c0 + lane;
-  uint32_t ph = (uint32_t)((ga + ((unsigned long long)c << 4) - g0) % R);
+  // phase of chunk c: its distance from g0 is below 2^32, so the remainder is 32-bit
+  uint32_t ph = ((c << 4) - (uint32_t)(g0 - ga)) % R;
   for (; c < c1; c += 32u) {
     st_out16(out + ga + ((unsigned long long)c << 4), t16[ph]);
     ph += step512;
@@ -1817,7 +1815,7 @@ __device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16
     b = g0 + lane;
     ok = b < gend;
   }
-  if (ok) out[b] = rs[(uint32_t)((b - g0) % R)];
+  if (ok) out[b] = rs[(uint32_t)(b - g0) % R];
 }
 
 // Input length, output range and super-tile count of the job described by p.
@@ -1911,6 +1909,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ unsigned long long s_frcnt[2];          // kModeFree: super-tile function (count, local carry-out)
   __shared__ long long s_frlco[2];
   __shared__ uint32_t s_supc[2][32], s_supx[2][32];  // kModeSmall: super-tile table over carries
+  __shared__ uint32_t s_noin[2];  // pass B of the super-tile reads no input (its loads are not queued)
+  __shared__ uint32_t s_phq[LoadRing::kPhases];
 
   const ReplaceParams& p = SEG ? s_job : pk;
   unsigned int* const sched = SEG ? sl.sched : &pk.res->tile_counter;  // claim counter, then finished CTAs
@@ -1964,7 +1964,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 
   // ---- load ring: thread 0 queues the loads of each pass in the order they are consumed
   LoadRing ring;
-  ring.init();
+  ring.init(s_phq);
 
   // pass A of super-tile t and its function (published as an aggregate record); tables in set `set`
   auto tile_front = [&](const uint32_t t, const uint32_t set) {
@@ -2051,13 +2051,32 @@ __global__ void __launch_bounds__(kThreads, 3)
     unsigned long long fr_cnt = 0;  // kModeFree: lane 0 of warp 1
     long long fr_lco = 0;
     uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 1, lane = carry-in
+    // Pass B reads no input when, in every warp region of a whole super-tile, the kept matches
+    // cover every byte (its output is a run of replacements, or nothing when R = 0) and fit
+    // the warp's staging: then every warp takes the table-driven path, and the super-tile's
+    // second loads, their waits and its per-sub-tile barriers are skipped. Free mode checks
+    // the carry 0 (full cover of the first region needs a match at byte 0, so no match
+    // of the previous super-tile can reach into it), small mode every carry into every region.
+    const bool whole = !SEG && m == nsub && tstart + S <= n && L <= 64u && (R == 0u || rep_table);
+    uint32_t noin = 0;
     if (MODE == kModeFree) {
       if (tid == 32u) {
+        bool ok = whole;
+        uint32_t csub_n = 0;
         for (uint32_t j = 0; j < m; ++j) {
           uint32_t tot_cnt = 0, tot_cend = 0;
           for (int w = 0; w < kWarps; ++w) {
-            tot_cnt += wcnt_s[j * kWarps + w];
+            const uint32_t wc = wcnt_s[j * kWarps + w];
             const uint32_t ce = wcend_s[j * kWarps + w];
+            if (ok) {
+              const uint32_t covs = csub_n > tot_cend ? csub_n : tot_cend;  // reach of the earlier warps
+              const uint32_t wlo = (uint32_t)w * 2048u;
+              uint32_t wcov = covs > wlo ? covs - wlo : 0u;
+              wcov = wcov < 2048u ? wcov : 2048u;
+              const uint32_t over = ce > wlo + 2048u ? ce - (wlo + 2048u) : 0u;
+              if (2048u - wcov - wc * L + over != 0u || wc * R + 15u > lay.wstage_cap) ok = false;
+            }
+            tot_cnt += wc;
             tot_cend = ce > tot_cend ? ce : tot_cend;
           }
           const long long lco = tot_cend > (uint32_t)kTile ? (long long)(tot_cend - kTile) : 0ll;
@@ -2065,12 +2084,17 @@ __global__ void __launch_bounds__(kThreads, 3)
           const long long shifted = fr_lco - (long long)kTile;
           fr_lco = shifted > lco ? shifted : lco;
           fr_cnt += tot_cnt;
+          const long long cs = (long long)csub_n - (long long)kTile;
+          const long long cn = cs > lco ? cs : lco;
+          csub_n = cn > 0 ? (uint32_t)cn : 0u;
         }
+        noin = ok ? 1u : 0u;
         if (t > 0)
           rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
       }
     } else if (warp == 1) {
       const uint32_t* wt = reinterpret_cast<const uint32_t*>(wtab_b);
+      bool bad = false;  // some region is not covered from some carry
       for (uint32_t j = 0; j < m; ++j) {
         uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
         uint32_t y = lane < L ? lane : 0u, cnt = 0;
@@ -2082,11 +2106,20 @@ __global__ void __launch_bounds__(kThreads, 3)
           y = v >> 16;
         }
         if (lane < L) (subrec_b)[j * L + lane] = (uint8_t)sup_carry;
+        if (whole && lane < L) {
+#pragma unroll
+          for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
+            const uint32_t v = wt[(j * kWarps + w) * L + lane];  // region w from carry `lane`
+            const uint32_t wc = v & 0xFFFFu, co = v >> 16;
+            if (2048u - lane - wc * L + co != 0u || wc * R + 15u > lay.wstage_cap) bad = true;
+          }
+        }
         const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
         const uint32_t tx = __shfl_sync(0xffffffffu, y, sup_carry);
         sup_cnt += tc;
         sup_carry = tx;
       }
+      noin = (whole && !__any_sync(0xffffffffu, bad)) ? 1u : 0u;
       if (use_rec) {
         unsigned long long e = lane < L ? ((unsigned long long)sup_cnt | ((unsigned long long)sup_carry << 17)) : 0ull;
         const unsigned long long e1 = __shfl_sync(0xffffffffu, e, 1), e2 = __shfl_sync(0xffffffffu, e, 2),
@@ -2107,15 +2140,30 @@ __global__ void __launch_bounds__(kThreads, 3)
       if (tid == 32u) {
         s_frcnt[set] = fr_cnt;
         s_frlco[set] = fr_lco;
+        s_noin[set] = noin;
       }
     } else if (warp == 1) {
       s_supc[set][lane] = sup_cnt;
       s_supx[set][lane] = sup_carry;
+      if (lane == 0) s_noin[set] = noin;
     }
   };
 
-  // look-back, pass B and records of super-tile t, whose pass A filled set `set`
-  auto tile_back = [&](const uint32_t t, const uint32_t set) {
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  // Thread 0, one apply: claim the next super-tile and queue its pass-A loads, then the pass-B
+  // loads of super-tile tcur (whose pass A filled set cset) unless its pass B reads no input.
+  auto schedule = [&](const uint32_t tcur, const uint32_t cset) {
+    const uint32_t c = atomicAdd(sched, 1u);
+    const uint32_t nx = c < NT ? c : kNone;
+    s_q[0] = nx;
+    if (nx != kNone) ring.push(nx, 0);
+    if (!s_noin[cset]) ring.push(tcur, 1);
+    ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+  };
+
+  // look-back, pass B and records of super-tile t, whose pass A filled set `set`; after the
+  // look-back, thread 0 schedules past super-tile tnext (set nset) when there is one
+  auto tile_back = [&](const uint32_t t, const uint32_t set, const uint32_t tnext, const uint32_t nset) {
     const uint32_t m = subs_in_tile(t, S, n, nsub);
     const unsigned long long tstart = (unsigned long long)t * S;
     uint64_t* const masks_s = masks + (size_t)set * nsub * kThreads;
@@ -2172,6 +2220,8 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
     __syncthreads();
+    if (tid == 0 && tnext != kNone) schedule(tnext, nset);
+    const bool noin = s_noin[set] != 0u;
     const uint32_t cin = s_cin;
     const unsigned long long kexcl = s_kexcl;
     const long long delta = (long long)R - (long long)L;
@@ -2185,7 +2235,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     uint32_t csub = cin;      // kModeFree: carry into sub-tile j
     long long last_abs = -1;  // last kept start seen by this thread
     for (uint32_t j = 0; j < m; ++j) {
-      uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
+      uint8_t* tb = noin ? smem + lay.in0 : ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
       const unsigned long long gseg = sstart + sb;
       const uint64_t mask = masks_s[j * kThreads + tid];
@@ -2234,29 +2284,23 @@ __global__ void __launch_bounds__(kThreads, 3)
       // ---- L <= 64: a warp whose output is a copy of its input or a run of replacements is
       // written straight from the pass-A tables, with no per-thread walk or scan
       uint32_t wbase = 0, sub_total = 0;
-      bool done = false;
+      bool done = false, fits0 = false;
       if (L <= 64u) {
         const uint32_t cut0 = __ballot_sync(0xffffffffu, lane < 8u && wbytes != 0u && wbytes < 2048u);
         if (!cut0) {
           lanes8_sum(wolen, &wbase, &sub_total);
           wbase = __shfl_sync(0xffffffffu, wbase, warp);
           sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
-          const bool fits0 = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
+          fits0 = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
           const bool stage0 =
               __reduce_max_sync(0xffffffffu, lane < 8u ? wolen : 0u) + 15u <= lay.wstage_cap;
           const uint32_t wcw = __shfl_sync(0xffffffffu, ewc, warp);
           const uint32_t wlw = __shfl_sync(0xffffffffu, wolen, warp);
           const uint32_t x0w = __shfl_sync(0xffffffffu, ewcov, warp);  // bytes covered at the region start
           // copy only (no kept start), nothing to write (all covered, R = 0), or replacements only
-          if (fits0 && !failed && stage0 && (wcw == 0u || wlw == 0u || (rep_table && wlw == wcw * R))) {
-            done = true;  // the same in every lane of the warp
-            if (wlw) {
-              if (wcw == 0u)
-                warp_emit_literal(p.out, tb, O + wbase, wlw, warp * 2048u + x0w);
-              else
-                warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512,
-                                  O + wbase, wlw);
-            }
+          const bool table_only = stage0 && (wcw == 0u || wlw == 0u || (rep_table && wlw == wcw * R));
+          if (table_only) {
+            // the last kept start, from the tables (also when nothing is written below)
             if (MODE == kModeFree) {
               if (mask) last_abs = (long long)(gseg + (63u - (uint32_t)__clzll((long long)mask)));
             } else if (wcw != 0u && lane == 0) {
@@ -2265,9 +2309,27 @@ __global__ void __launch_bounds__(kThreads, 3)
               last_abs = (long long)(sstart + warp * 2048u + x0w + (unsigned long long)(wcw - 1u) * L);
             }
           }
+          if (fits0 && !failed && table_only) {
+            done = true;  // the same in every lane of the warp
+            if (wlw) {
+              if (wcw == 0u)
+                warp_emit_literal(p.out, tb, O + wbase, wlw, warp * 2048u + x0w);
+              else
+                warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512,
+                                  O + wbase, wlw);
+            }
+          }
         }
       }
-      if (!done) {
+      if (!done && noin) {
+        // no input here: every region was shown to take the path above; only an output that
+        // does not fit (reported, nothing written) or a failed look-back can bring a warp here
+        if (!fits0) {
+          if (tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
+        } else if (!failed) {
+          set_error(p);
+        }
+      } else if (!done) {
       if (MODE == kModeFree) {
         if (L <= 64u) {
           // only the previous segment's last match (or the sub-tile carry) can reach here
@@ -2481,9 +2543,11 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       }  // !done
       O += sub_total;
-      __syncthreads();
-      ring.release();
-      if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+      if (!noin) {
+        __syncthreads();
+        ring.release();
+        if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+      }
     }
 
     // ================= per-super-tile records: last kept start, totals
@@ -2512,7 +2576,6 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
   };
 
-  constexpr uint32_t kNone = 0xFFFFFFFFu;
   if (tid == 0) {
     for (int b = 0; b < kNBuf; ++b) mbar_init(&s_bar[b], 1);
     fence_mbar_init();
@@ -2550,7 +2613,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       tile_front(t, 0);
       __syncthreads();  // the fold (warp 1) is done before this super-tile's look-back (warp 0)
-      tile_back(t, 0);
+      tile_back(t, 0, kNone, 0);
       // claim the next super-tile only now, when its pass A starts: a super-tile claimed
       // early but started late would hold up the look-back of every later super-tile
       if (tid == 0) {
@@ -2566,26 +2629,20 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
   } else {
     // one apply: pass A of super-tile k runs while super-tile k-1's predecessors publish
-    // their records; then k-1 looks back (its wait mostly over) and writes its output. A
-    // super-tile is still claimed when its pass A starts, so every claimed super-tile
-    // publishes its aggregate without waiting on another CTA.
+    // their records; then k-1 looks back (its wait mostly over) and writes its output. The
+    // next super-tile is claimed right after that look-back, so its pass-A loads stream in
+    // during k-1's pass B, and it still publishes its aggregate without waiting on another CTA.
     uint32_t tprev = kNone, k = 0;
     for (;;) {
       __syncthreads();
       const uint32_t tcur = s_q[0];
       if (tcur == kNone && tprev == kNone) break;
       if (tcur != kNone) tile_front(tcur, k & 1u);
-      if (tprev != kNone) tile_back(tprev, (k & 1u) ^ 1u);
-      if (tid == 0) {
-        uint32_t nx = kNone;
-        if (tcur != kNone) {
-          const uint32_t c = atomicAdd(sched, 1u);
-          nx = c < NT ? c : kNone;
-        }
-        s_q[0] = nx;
-        if (nx != kNone) ring.push(nx, 0);
-        if (tcur != kNone) ring.push(tcur, 1);
-        ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+      if (tprev != kNone) {
+        tile_back(tprev, (k & 1u) ^ 1u, tcur, k & 1u);
+      } else if (tcur != kNone) {
+        __syncthreads();  // the fold's flags of tcur are visible to thread 0
+        if (tid == 0) schedule(tcur, k & 1u);
       }
       tprev = tcur;
       ++k;

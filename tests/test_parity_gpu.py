@@ -91,6 +91,24 @@ def test_periodic_runs_across_tiles(cr_lib, pat):
                     assert s.result() == src.replace(pat, rep), (n, base, pat[:8], len(pat), rep)
 
 
+def test_runs_with_sparse_breaks(cr_lib):
+    """Multi-MB runs broken at a few random places: most 64 KiB super-tiles are covered by
+    kept matches end to end (pass B writes them from the tables alone), the broken ones and
+    their neighbours are not; every carry across the breaks has to line up."""
+    rng = random.Random(77)
+    for base, pats in ((b"a", (b"a", b"aa", b"aaa", b"a" * 5, b"a" * 32, b"a" * 33)),
+                       (b"ab", (b"ab", b"abab", b"aba", b"b"))):
+        n = 3_000_017
+        src = bytearray((base * (n // len(base) + 1))[:n])
+        for _ in range(25):
+            i = rng.randrange(n)
+            src[i:i + 1] = rng.choice((b"c", b"b", b"a"))
+        src = bytes(src)
+        for pat in pats:
+            for rep in (b"", b"X", b"QRS", b"0123456789" * 3):
+                assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (base, pat, rep)
+
+
 def test_tile_boundary_straddles(cr_lib):
     rng = random.Random(5)
     for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
