@@ -1789,18 +1789,28 @@ __device__ __forceinline__ void warp_emit_literal(uint8_t* out, const uint8_t* t
   if (ok) out[b] = tb[srcw + (uint32_t)(b - g0)];
 }
 
+// x mod R for x < 2^17 and 1 <= R <= 64, with rmag = ceil(2^32 / R) (0 for R = 1): the
+// quotient is the high word of x * rmag (its error, below x / 2^32, stays under 1/R).
+__host__ __device__ __forceinline__ uint32_t mod_magic(uint32_t R) {
+  return R > 1u ? (uint32_t)((0x100000000ull + R - 1u) / R) : 0u;
+}
+__device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t R, uint32_t rmag) {
+  return R > 1u ? x - __umulhi(x, rmag) * R : 0u;
+}
+
 // One warp's output when it is a run of replacements: 16 bytes per phase from the table t16
 // (the replacement repeated from every phase), the partial chunks from rs byte by byte.
 __device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16, const uint8_t* rs, uint32_t R,
-                                                  uint32_t step512, unsigned long long g0, uint32_t wtot) {
+                                                  uint32_t step512, uint32_t rmag, unsigned long long g0,
+                                                  uint32_t wtot) {
   const uint32_t lane = threadIdx.x & 31u;
   const unsigned long long ga = g0 & ~15ull;
   const unsigned long long gend = g0 + wtot;
   const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);
   const uint32_t c1 = (uint32_t)((gend - ga) >> 4);
   uint32_t c = c0 + lane;
-  // phase of chunk c: its distance from g0 is below 2^32, so the remainder is 32-bit
-  uint32_t ph = ((c << 4) - (uint32_t)(g0 - ga)) % R;
+  // phase of chunk c: its distance from g0 (below 2^17) modulo R
+  uint32_t ph = mod_small(((c << 4) - (uint32_t)(g0 - ga)), R, rmag);
   for (; c < c1; c += 32u) {
     st_out16(out + ga + ((unsigned long long)c << 4), t16[ph]);
     ph += step512;
@@ -1815,7 +1825,7 @@ __device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16
     b = g0 + lane;
     ok = b < gend;
   }
-  if (ok) out[b] = rs[(uint32_t)(b - g0) % R];
+  if (ok) out[b] = rs[mod_small((uint32_t)(b - g0), R, rmag)];
 }
 
 // Input length, output range and super-tile count of the job described by p.
@@ -1925,7 +1935,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   const uint32_t sb = tid * kSeg;
   const unsigned long long S = (unsigned long long)nsub * kTile;
   // the job's dimensions and pattern: once (one apply) or whenever the job changes (segmented)
-  uint32_t L = 0, R = 0, NT = 0, carry0 = 0, want_a = 0, step4 = 0, step512 = 0;
+  uint32_t L = 0, R = 0, NT = 0, carry0 = 0, want_a = 0, step4 = 0, step512 = 0, rmag = 0;
   unsigned long long n_all = 0, n = 0, n16 = 0;
   bool rep_table = false;
   auto setup_job = [&]() {
@@ -1941,6 +1951,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     rep_table = R >= 1u && R <= 64u;
     step4 = R ? 4u % R : 0u;
     step512 = R ? 512u % R : 0u;
+    rmag = mod_magic(R);
     const uint8_t* psrc = (!SEG && L <= (uint32_t)kInlineMax) ? p.pat : p.pat_ext;
     const uint8_t* rsrc = (!SEG && R <= (uint32_t)kInlineMax) ? p.rep : p.rep_ext;
     for (uint32_t i = tid; i < L; i += kThreads) ps[i] = psrc[i];
@@ -2052,12 +2063,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     long long fr_lco = 0;
     uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 1, lane = carry-in
     // Pass B reads no input when, in every warp region of a whole super-tile, the kept matches
-    // cover every byte (its output is a run of replacements, or nothing when R = 0) and fit
-    // the warp's staging: then every warp takes the table-driven path, and the super-tile's
-    // second loads, their waits and its per-sub-tile barriers are skipped. Free mode checks
+    // cover every byte (its output is a run of replacements, or nothing when R = 0): then the
+    // tables alone place and write the output, and the super-tile's second loads, their waits
+    // and its per-sub-tile barriers are skipped. Free mode checks
     // the carry 0 (full cover of the first region needs a match at byte 0, so no match
     // of the previous super-tile can reach into it), small mode every carry into every region.
-    const bool whole = !SEG && m == nsub && tstart + S <= n && L <= 64u && (R == 0u || rep_table);
+    const bool whole = !SEG && m == nsub && nsub * kWarps <= 32u && tstart + S <= n && L <= 64u &&
+                       (R == 0u || rep_table);
     uint32_t noin = 0;
     if (MODE == kModeFree) {
       if (tid == 32u) {
@@ -2074,7 +2086,7 @@ __global__ void __launch_bounds__(kThreads, 3)
               uint32_t wcov = covs > wlo ? covs - wlo : 0u;
               wcov = wcov < 2048u ? wcov : 2048u;
               const uint32_t over = ce > wlo + 2048u ? ce - (wlo + 2048u) : 0u;
-              if (2048u - wcov - wc * L + over != 0u || wc * R + 15u > lay.wstage_cap) ok = false;
+              if (2048u - wcov - wc * L + over != 0u) ok = false;
             }
             tot_cnt += wc;
             tot_cend = ce > tot_cend ? ce : tot_cend;
@@ -2111,7 +2123,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
             const uint32_t v = wt[(j * kWarps + w) * L + lane];  // region w from carry `lane`
             const uint32_t wc = v & 0xFFFFu, co = v >> 16;
-            if (2048u - lane - wc * L + co != 0u || wc * R + 15u > lay.wstage_cap) bad = true;
+            if (2048u - lane - wc * L + co != 0u) bad = true;
           }
         }
         const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
@@ -2231,11 +2243,82 @@ __global__ void __launch_bounds__(kThreads, 3)
                                                              (long long)kexcl * delta);
     const bool failed = s_fail != 0;
 
+    // ================= pass B, no input: every warp region of this whole super-tile is a run of
+    // replacements or empty. Lane r stands for region r % 8 of sub-tile r / 8: its output length
+    // from the tables, a scan over the 32 lanes places it, and each warp writes its region of
+    // every sub-tile. The last kept start follows from the regions (kept starts x0, x0 + L, ...).
+    uint32_t noin_last1 = 0;
+    if (noin) {
+      const uint32_t jr = lane >> 3, wr = lane & 7u;
+      uint32_t wc = 0, x0 = 0, olen_r = 0, we = 0;
+      if (MODE == kModeFree && jr < m) {
+        wc = wcnt_s[lane];  // index jr * kWarps + wr
+        we = wcend_s[lane];
+      }
+      uint32_t pre = we;  // kModeFree: max cover end of the earlier regions of the same sub-tile
+      if (MODE == kModeFree) {
+#pragma unroll
+        for (int d = 1; d < 8; d <<= 1) {
+          const uint32_t o = __shfl_up_sync(0xffffffffu, pre, d, 8);
+          if (wr >= (uint32_t)d) pre = o > pre ? o : pre;
+        }
+        pre = __shfl_up_sync(0xffffffffu, pre, 1, 8);
+      }
+      if (jr < m) {
+        if (MODE == kModeFree) {
+          // carry into sub-tile jr: cin, then the previous sub-tile's reach (L <= 64, so a cover
+          // never spans a whole sub-tile)
+          const uint32_t csj = jr == 0 ? cin : sublco_s[jr - 1];
+          const uint32_t ex = wr == 0 ? 0u : pre;
+          const uint32_t covs = csj > ex ? csj : ex;
+          const uint32_t wlo = wr * 2048u;
+          uint32_t wcov = covs > wlo ? covs - wlo : 0u;
+          wcov = wcov < 2048u ? wcov : 2048u;
+          const uint32_t over = we > wlo + 2048u ? we - (wlo + 2048u) : 0u;
+          olen_r = 2048u - wcov - wc * L + over + wc * R;
+          x0 = wcov;
+        } else {
+          const uint32_t cs = subrec_b[jr * L + cin];
+          const uint32_t cw = wrec_b[(jr * kWarps + wr) * L + cs];
+          const uint32_t e = reinterpret_cast<const uint32_t*>(wtab_b)[(jr * kWarps + wr) * L + cw];
+          wc = e & 0xFFFFu;
+          olen_r = 2048u - cw - wc * L + (e >> 16) + wc * R;
+          x0 = cw;
+        }
+      }
+      uint32_t incl = olen_r;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= (uint32_t)d) incl += o;
+      }
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      const uint32_t offr = incl - olen_r;
+      noin_last1 = __reduce_max_sync(0xffffffffu, wc ? jr * (uint32_t)kTile + wr * 2048u + x0 + (wc - 1u) * L + 1u : 0u);
+      const bool lit = __any_sync(0xffffffffu, olen_r != wc * R);  // a literal byte: not shown by the fold
+      const bool fits_t = (O + total <= p.out_cap) && (O <= p.out_cap);
+      if (!fits_t) {
+        if (tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
+      } else if (lit) {
+        if (tid == 0) set_error(p);
+      } else if (!failed) {
+        for (uint32_t j = 0; j < m; ++j) {
+          const uint32_t r = j * kWarps + warp;
+          const uint32_t ol = __shfl_sync(0xffffffffu, olen_r, r);
+          const uint32_t of = __shfl_sync(0xffffffffu, offr, r);
+          if (ol)
+            warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, rmag,
+                              O + of, ol);
+        }
+      }
+      O += total;
+    }
+
     // ================= pass B: exact kept starts and output, one warp region at a time
     uint32_t csub = cin;      // kModeFree: carry into sub-tile j
     long long last_abs = -1;  // last kept start seen by this thread
-    for (uint32_t j = 0; j < m; ++j) {
-      uint8_t* tb = noin ? smem + lay.in0 : ring.wait(p, smem, lay, s_bar, &s_fail);
+    for (uint32_t j = 0; j < (noin ? 0u : m); ++j) {
+      uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
       const unsigned long long gseg = sstart + sb;
       const uint64_t mask = masks_s[j * kThreads + tid];
@@ -2284,14 +2367,14 @@ __global__ void __launch_bounds__(kThreads, 3)
       // ---- L <= 64: a warp whose output is a copy of its input or a run of replacements is
       // written straight from the pass-A tables, with no per-thread walk or scan
       uint32_t wbase = 0, sub_total = 0;
-      bool done = false, fits0 = false;
+      bool done = false;
       if (L <= 64u) {
         const uint32_t cut0 = __ballot_sync(0xffffffffu, lane < 8u && wbytes != 0u && wbytes < 2048u);
         if (!cut0) {
           lanes8_sum(wolen, &wbase, &sub_total);
           wbase = __shfl_sync(0xffffffffu, wbase, warp);
           sub_total = __shfl_sync(0xffffffffu, sub_total, 7);
-          fits0 = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
+          const bool fits0 = (O + sub_total <= p.out_cap) && (O <= p.out_cap);
           const bool stage0 =
               __reduce_max_sync(0xffffffffu, lane < 8u ? wolen : 0u) + 15u <= lay.wstage_cap;
           const uint32_t wcw = __shfl_sync(0xffffffffu, ewc, warp);
@@ -2316,20 +2399,12 @@ __global__ void __launch_bounds__(kThreads, 3)
                 warp_emit_literal(p.out, tb, O + wbase, wlw, warp * 2048u + x0w);
               else
                 warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512,
-                                  O + wbase, wlw);
+                                  rmag, O + wbase, wlw);
             }
           }
         }
       }
-      if (!done && noin) {
-        // no input here: every region was shown to take the path above; only an output that
-        // does not fit (reported, nothing written) or a failed look-back can bring a warp here
-        if (!fits0) {
-          if (tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
-        } else if (!failed) {
-          set_error(p);
-        }
-      } else if (!done) {
+      if (!done) {
       if (MODE == kModeFree) {
         if (L <= 64u) {
           // only the previous segment's last match (or the sub-tile carry) can reach here
@@ -2409,7 +2484,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           warp_emit_literal(p.out, tb, O + wbase, wtot, warp * 2048u + __shfl_sync(0xffffffffu, x_in, 0));
         } else {
           // ---- REPLACE: output = the replacement repeated
-          warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, O + wbase,
+          warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, rmag, O + wbase,
                             wtot);
         }
       } else if (fits && !failed && warp_stage) {
@@ -2543,18 +2618,16 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       }  // !done
       O += sub_total;
-      if (!noin) {
-        __syncthreads();
-        ring.release();
-        if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
-      }
+      __syncthreads();
+      ring.release();
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
     }
 
     // ================= per-super-tile records: last kept start, totals
     {
       const uint32_t last1 = last_abs >= 0 ? (uint32_t)((unsigned long long)last_abs - tstart + 1) : 0u;
-      uint32_t tot_last1;
-      (void)block_excl_scan1(last1, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot_last1);
+      uint32_t tot_last1 = noin_last1;  // no input: the same in every thread already
+      if (!noin) (void)block_excl_scan1(last1, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot_last1);
       if (tid == 0) {
         const long long lastt = tot_last1 ? (long long)(tstart + tot_last1 - 1) : -1ll;
         __stcg(p.tile_last + t, lastt);
