@@ -1463,10 +1463,53 @@ __device__ __forceinline__ uint32_t tab4_entry(unsigned long long d0, unsigned l
   return (uint32_t)((c & 1u) ? (w >> 19) : w) & 0x7FFFFu;
 }
 
-__device__ __forceinline__ bool lookback_small4_rec(const ReplaceParams& p, uint32_t t, uint32_t L,
-                                                    unsigned long long* K_out, uint32_t* c_out, uint32_t carry0) {
+// Functions over carries 0..LL-1 (patterns of LL <= 4 bytes) with wide counts, one register
+// per entry: kept count in bits 0-23, carry-out in bits 24-31.
+template <int LL>
+__device__ __forceinline__ uint32_t fn_at(const uint32_t g[4], uint32_t k) {
+  if (LL == 2) return k == 0u ? g[0] : g[1];
+  if (LL == 3) return k == 0u ? g[0] : (k == 1u ? g[1] : g[2]);
+  return k == 0u ? g[0] : (k == 1u ? g[1] : (k == 2u ? g[2] : g[3]));
+}
+// g := g applied after o (o covers the earlier bytes)
+template <int LL>
+__device__ __forceinline__ void fn_after(uint32_t g[4], const uint32_t o[4]) {
+  uint32_t r[4];
+#pragma unroll
+  for (int y = 0; y < LL; ++y) {
+    const uint32_t m = fn_at<LL>(g, o[y] >> 24);
+    r[y] = ((o[y] & 0xFFFFFFu) + (m & 0xFFFFFFu)) | (m & 0xFF000000u);
+  }
+#pragma unroll
+  for (int y = 0; y < LL; ++y) g[y] = r[y];
+}
+// One step of an inclusive scan of functions over lanes, earlier bytes in lower lanes: within
+// groups of `width` lanes (pos: the lane's place in its group) or across groups (width 32).
+template <int LL>
+__device__ __forceinline__ void fn_scan_up(uint32_t g[4], uint32_t step, uint32_t width, uint32_t pos) {
+  uint32_t o[4];
+#pragma unroll
+  for (int y = 0; y < LL; ++y) o[y] = __shfl_up_sync(0xffffffffu, g[y], step, width);
+  if (pos >= step) fn_after<LL>(g, o);
+}
+// The same with earlier bytes in higher lanes.
+template <int LL>
+__device__ __forceinline__ void fn_scan_down(uint32_t g[4], uint32_t step) {
+  uint32_t o[4];
+#pragma unroll
+  for (int y = 0; y < LL; ++y) o[y] = __shfl_down_sync(0xffffffffu, g[y], step);
+  if ((threadIdx.x & 31u) + step < 32u) fn_after<LL>(g, o);
+}
+
+// Look-back for patterns of LL <= 4 bytes over the 16-byte records. Each window of 32
+// predecessors is composed by a scan over lanes (lane l: super-tile t - 1 - l, the identity at
+// and beyond the nearest inclusive one), so a window costs a few shuffle steps whatever its
+// length.
+template <int LL>
+__device__ __forceinline__ bool lookback_small_rec(const ReplaceParams& p, uint32_t t, unsigned long long* K_out,
+                                                   uint32_t* c_out, uint32_t carry0) {
   const uint32_t lane = threadIdx.x & 31u;
-  unsigned long long acc_cnt = 0;  // lane c < L: function of the tiles between the window and t
+  unsigned long long acc_cnt = 0;  // lane c < LL: function of the super-tiles between the window and t
   uint32_t acc_carry = lane;
   long long base = (long long)t - 1;
   for (;;) {
@@ -1474,38 +1517,88 @@ __device__ __forceinline__ bool lookback_small4_rec(const ReplaceParams& p, uint
     const int plr = warp_read_window(p, base, &d0, &d1, carry0);
     if (plr < 0) return false;
     const uint32_t pl = (uint32_t)plr;
-    if (pl < 32) {
-      unsigned long long K = __shfl_sync(0xffffffffu, d0, pl);
-      uint32_t x = (uint32_t)__shfl_sync(0xffffffffu, d1, pl);
+    uint32_t g[4];
 #pragma unroll
-      for (int i = 31; i >= 0; --i) {
-        if ((uint32_t)i < pl) {
-          const unsigned long long a = __shfl_sync(0xffffffffu, d0, i);
-          const unsigned long long b = __shfl_sync(0xffffffffu, d1, i);
-          const uint32_t e = tab4_entry(a, b, x);
-          K += e & 0x1FFFFu;
-          x = e >> 17;
-        }
+    for (uint32_t y = 0; y < (uint32_t)LL; ++y) {
+      g[y] = y << 24;
+      if (lane < pl) {
+        const uint32_t e = tab4_entry(d0, d1, y);
+        g[y] = (e & 0x1FFFFu) | ((e >> 17) << 24);
       }
-      *K_out = K + __shfl_sync(0xffffffffu, acc_cnt, x);
-      *c_out = __shfl_sync(0xffffffffu, acc_carry, x);
+    }
+    fn_scan_down<LL>(g, 1);
+    fn_scan_down<LL>(g, 2);
+    fn_scan_down<LL>(g, 4);
+    fn_scan_down<LL>(g, 8);
+    fn_scan_down<LL>(g, 16);
+    // lane 0 now holds the window's function (its oldest super-tile applied first)
+    if (pl < 32) {
+      const unsigned long long K = __shfl_sync(0xffffffffu, d0, pl);  // the inclusive one
+      const uint32_t x = (uint32_t)__shfl_sync(0xffffffffu, d1, pl);
+      const uint32_t e = __shfl_sync(0xffffffffu, fn_at<LL>(g, x), 0);
+      const uint32_t xc = e >> 24;
+      *K_out = K + (e & 0xFFFFFFu) + __shfl_sync(0xffffffffu, acc_cnt, xc);
+      *c_out = __shfl_sync(0xffffffffu, acc_carry, xc);
       return true;
     }
-    uint32_t y = lane < L ? lane : 0u;
-    unsigned long long wc = 0;
+    uint32_t w[4];
 #pragma unroll
-    for (int i = 31; i >= 0; --i) {
-      const unsigned long long a = __shfl_sync(0xffffffffu, d0, i);
-      const unsigned long long b = __shfl_sync(0xffffffffu, d1, i);
-      const uint32_t e = tab4_entry(a, b, y);
-      wc += e & 0x1FFFFu;
-      y = e >> 17;
-    }
+    for (uint32_t y = 0; y < (uint32_t)LL; ++y) w[y] = __shfl_sync(0xffffffffu, g[y], 0);
+    const uint32_t e = fn_at<LL>(w, lane < (uint32_t)LL ? lane : 0u);  // entry `lane` of the window
+    const uint32_t y = e >> 24;
     const unsigned long long ac = __shfl_sync(0xffffffffu, acc_cnt, y);
     const uint32_t ax = __shfl_sync(0xffffffffu, acc_carry, y);
-    acc_cnt = wc + ac;
+    acc_cnt = (e & 0xFFFFFFu) + ac;
     acc_carry = ax;
     base -= 32;
+  }
+}
+
+// Fold of a super-tile of m <= 4 sub-tiles for patterns of LL <= 4 bytes (warp 1): lane r
+// holds the function of warp region r % 8 of sub-tile r / 8 (idle lanes: the identity). Scans
+// over each group of 8 lanes give the carry into every region from its sub-tile's carry-in
+// (wrec), scans over the sub-tile functions the carry into every sub-tile from the
+// super-tile's carry-in (subrec) and the super-tile function (entry `lane`). bad: some region
+// is not covered end to end from some carry (checked when `whole`).
+template <int LL>
+__device__ __forceinline__ void fold_small_rec(const uint32_t* wt, uint8_t* wrec, uint8_t* subrec, uint32_t m,
+                                               bool whole, bool* bad, uint32_t* sup_cnt, uint32_t* sup_carry) {
+  const uint32_t lane = threadIdx.x & 31u, jr = lane >> 3, wr = lane & 7u;
+  const bool act = jr < m;
+  uint32_t g[4];
+#pragma unroll
+  for (uint32_t y = 0; y < (uint32_t)LL; ++y) {
+    g[y] = y << 24;
+    if (act) {
+      const uint32_t v = wt[lane * LL + y];
+      const uint32_t wc = v & 0xFFFFu, co = v >> 16;
+      g[y] = wc | (co << 24);
+      if (whole && 2048u - y - wc * LL + co != 0u) *bad = true;
+    }
+  }
+  fn_scan_up<LL>(g, 1, 8, wr);
+  fn_scan_up<LL>(g, 2, 8, wr);
+  fn_scan_up<LL>(g, 4, 8, wr);
+  uint32_t h[4];
+#pragma unroll
+  for (uint32_t y = 0; y < (uint32_t)LL; ++y) {
+    uint32_t x = __shfl_up_sync(0xffffffffu, g[y], 1, 8);
+    if (wr == 0) x = y << 24;
+    if (act) wrec[lane * LL + y] = (uint8_t)(x >> 24);
+    h[y] = __shfl_sync(0xffffffffu, g[y], lane | 7u);  // the sub-tile's function
+  }
+  fn_scan_up<LL>(h, 8, 32, lane);
+  fn_scan_up<LL>(h, 16, 32, lane);
+#pragma unroll
+  for (uint32_t y = 0; y < (uint32_t)LL; ++y) {
+    uint32_t xe = __shfl_up_sync(0xffffffffu, h[y], 8);
+    if (jr == 0) xe = y << 24;
+    if (act && wr == 0) subrec[jr * LL + y] = (uint8_t)(xe >> 24);
+    const uint32_t e = __shfl_sync(0xffffffffu, h[y], 31);  // entry y of the super-tile function
+    if (lane == y) {
+      *sup_cnt = e & 0xFFFFFFu;
+      *sup_carry = e >> 24;
+    }
   }
 }
 
@@ -2072,41 +2165,67 @@ __global__ void __launch_bounds__(kThreads, 3)
                        (R == 0u || rep_table);
     uint32_t noin = 0;
     if (MODE == kModeFree) {
-      if (tid == 32u) {
-        bool ok = whole;
-        uint32_t csub_n = 0;
-        for (uint32_t j = 0; j < m; ++j) {
-          uint32_t tot_cnt = 0, tot_cend = 0;
-          for (int w = 0; w < kWarps; ++w) {
-            const uint32_t wc = wcnt_s[j * kWarps + w];
-            const uint32_t ce = wcend_s[j * kWarps + w];
-            if (ok) {
-              const uint32_t covs = csub_n > tot_cend ? csub_n : tot_cend;  // reach of the earlier warps
-              const uint32_t wlo = (uint32_t)w * 2048u;
-              uint32_t wcov = covs > wlo ? covs - wlo : 0u;
-              wcov = wcov < 2048u ? wcov : 2048u;
-              const uint32_t over = ce > wlo + 2048u ? ce - (wlo + 2048u) : 0u;
-              if (2048u - wcov - wc * L + over != 0u) ok = false;
-            }
-            tot_cnt += wc;
-            tot_cend = ce > tot_cend ? ce : tot_cend;
+      if (warp == 1) {
+        // lane r stands for warp region r % 8 of sub-tile j0 + r / 8 (groups of 8 lanes)
+        const uint32_t wr = lane & 7u;
+        bool ok = whole;  // whole: m <= 4, one round
+        uint32_t cnt_sum = 0;
+        long long lco_max = LLONG_MIN;
+        for (uint32_t j0 = 0; j0 < m; j0 += 4u) {
+          const uint32_t jr = j0 + (lane >> 3);
+          const bool act = jr < m;
+          const uint32_t wc = act ? wcnt_s[jr * kWarps + wr] : 0u;
+          const uint32_t ce = act ? wcend_s[jr * kWarps + wr] : 0u;
+          uint32_t gmax = ce, pre = ce;  // sub-tile max reach; inclusive max over earlier regions
+#pragma unroll
+          for (int d = 1; d < 8; d <<= 1) {
+            const uint32_t x = __shfl_xor_sync(0xffffffffu, gmax, d, 8);
+            gmax = x > gmax ? x : gmax;
+            const uint32_t o = __shfl_up_sync(0xffffffffu, pre, d, 8);
+            if (wr >= (uint32_t)d) pre = o > pre ? o : pre;
           }
-          const long long lco = tot_cend > (uint32_t)kTile ? (long long)(tot_cend - kTile) : 0ll;
-          sublco_s[j] = (uint32_t)lco;
-          const long long shifted = fr_lco - (long long)kTile;
-          fr_lco = shifted > lco ? shifted : lco;
-          fr_cnt += tot_cnt;
-          const long long cs = (long long)csub_n - (long long)kTile;
-          const long long cn = cs > lco ? cs : lco;
-          csub_n = cn > 0 ? (uint32_t)cn : 0u;
+          pre = __shfl_up_sync(0xffffffffu, pre, 1, 8);
+          if (wr == 0) pre = 0;
+          const uint32_t lco = gmax > (uint32_t)kTile ? gmax - (uint32_t)kTile : 0u;  // reach past the sub-tile
+          if (act && wr == 0) sublco_s[jr] = lco;
+          cnt_sum += __reduce_add_sync(0xffffffffu, wc);
+          // the super-tile's reach: max over sub-tiles of their reach, less the sub-tiles after them
+          const long long v = act ? (long long)lco - (long long)(m - 1u - jr) * kTile : LLONG_MIN;
+          lco_max = v > lco_max ? v : lco_max;
+          if (ok) {
+            // carry into the sub-tile from carry 0: the previous sub-tile's reach (L <= 64)
+            uint32_t csj = __shfl_up_sync(0xffffffffu, lco, 8);
+            if (jr == 0) csj = 0;
+            const uint32_t covs = csj > pre ? csj : pre;  // reach of everything before the region
+            const uint32_t wlo = wr * 2048u;
+            uint32_t wcov = covs > wlo ? covs - wlo : 0u;
+            wcov = wcov < 2048u ? wcov : 2048u;
+            const uint32_t over = ce > wlo + 2048u ? ce - (wlo + 2048u) : 0u;
+            ok = __all_sync(0xffffffffu, !act || 2048u - wcov - wc * L + over == 0u);
+          }
         }
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+          const long long o = __shfl_xor_sync(0xffffffffu, lco_max, d);
+          lco_max = o > lco_max ? o : lco_max;
+        }
+        fr_cnt = cnt_sum;
+        fr_lco = lco_max;
         noin = ok ? 1u : 0u;
-        if (t > 0)
+        if (lane == 0 && t > 0)
           rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
       }
     } else if (warp == 1) {
       const uint32_t* wt = reinterpret_cast<const uint32_t*>(wtab_b);
       bool bad = false;  // some region is not covered from some carry
+      if (use_rec && m <= 4u) {
+        if (L == 2u)
+          fold_small_rec<2>(wt, wrec_b, subrec_b, m, whole, &bad, &sup_cnt, &sup_carry);
+        else if (L == 3u)
+          fold_small_rec<3>(wt, wrec_b, subrec_b, m, whole, &bad, &sup_cnt, &sup_carry);
+        else
+          fold_small_rec<4>(wt, wrec_b, subrec_b, m, whole, &bad, &sup_cnt, &sup_carry);
+      } else
       for (uint32_t j = 0; j < m; ++j) {
         uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
         uint32_t y = lane < L ? lane : 0u, cnt = 0;
@@ -2196,8 +2315,12 @@ __global__ void __launch_bounds__(kThreads, 3)
       if (t > 0) {
         if (MODE == kModeFree)
           ok = lookback_free_rec(p, t, S, &K, &c, carry0);
-        else if (use_rec)
-          ok = lookback_small4_rec(p, t, L, &K, &c, carry0);
+        else if (L == 2u)
+          ok = lookback_small_rec<2>(p, t, &K, &c, carry0);
+        else if (L == 3u)
+          ok = lookback_small_rec<3>(p, t, &K, &c, carry0);
+        else if (L == 4u)
+          ok = lookback_small_rec<4>(p, t, &K, &c, carry0);
         else
           ok = lookback_small(p, t, L, &K, &c, carry0);
       }
