@@ -1558,11 +1558,13 @@ __device__ __forceinline__ bool lookback_small_rec(const ReplaceParams& p, uint3
 // holds the function of warp region r % 8 of sub-tile r / 8 (idle lanes: the identity). Scans
 // over each group of 8 lanes give the carry into every region from its sub-tile's carry-in
 // (wrec), scans over the sub-tile functions the carry into every sub-tile from the
-// super-tile's carry-in (subrec) and the super-tile function (entry `lane`). bad: some region
-// is not covered end to end from some carry (checked when `whole`).
+// super-tile's carry-in (subrec) and the super-tile function (entry `lane`). Checked when
+// `whole`: some region is not covered end to end from some carry (*bad), or is neither covered
+// nor free of kept starts (*mixed).
 template <int LL>
 __device__ __forceinline__ void fold_small_rec(const uint32_t* wt, uint8_t* wrec, uint8_t* subrec, uint32_t m,
-                                               bool whole, bool* bad, uint32_t* sup_cnt, uint32_t* sup_carry) {
+                                               bool whole, bool* bad, bool* mixed, uint32_t* sup_cnt,
+                                               uint32_t* sup_carry) {
   const uint32_t lane = threadIdx.x & 31u, jr = lane >> 3, wr = lane & 7u;
   const bool act = jr < m;
   uint32_t g[4];
@@ -1573,7 +1575,10 @@ __device__ __forceinline__ void fold_small_rec(const uint32_t* wt, uint8_t* wrec
       const uint32_t v = wt[lane * LL + y];
       const uint32_t wc = v & 0xFFFFu, co = v >> 16;
       g[y] = wc | (co << 24);
-      if (whole && 2048u - y - wc * LL + co != 0u) *bad = true;
+      if (whole && 2048u - y - wc * LL + co != 0u) {
+        *bad = true;
+        if (wc != 0u) *mixed = true;
+      }
     }
   }
   fn_scan_up<LL>(g, 1, 8, wr);
@@ -1882,7 +1887,7 @@ __device__ __forceinline__ void warp_emit_literal(uint8_t* out, const uint8_t* t
   if (ok) out[b] = tb[srcw + (uint32_t)(b - g0)];
 }
 
-// x mod R for x < 2^17 and 1 <= R <= 64, with rmag = ceil(2^32 / R) (0 for R = 1): the
+// x mod R for x < 2^26 and 1 <= R <= 64, with rmag = ceil(2^32 / R) (0 for R = 1): the
 // quotient is the high word of x * rmag (its error, below x / 2^32, stays under 1/R).
 __host__ __device__ __forceinline__ uint32_t mod_magic(uint32_t R) {
   return R > 1u ? (uint32_t)((0x100000000ull + R - 1u) / R) : 0u;
@@ -1895,19 +1900,24 @@ __device__ __forceinline__ uint32_t mod_small(uint32_t x, uint32_t R, uint32_t r
 // (the replacement repeated from every phase), the partial chunks from rs byte by byte.
 __device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16, const uint8_t* rs, uint32_t R,
                                                   uint32_t step512, uint32_t rmag, unsigned long long g0,
-                                                  uint32_t wtot) {
+                                                  uint32_t wtot, uint32_t ph0 = 0) {
   const uint32_t lane = threadIdx.x & 31u;
   const unsigned long long ga = g0 & ~15ull;
   const unsigned long long gend = g0 + wtot;
   const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);
   const uint32_t c1 = (uint32_t)((gend - ga) >> 4);
   uint32_t c = c0 + lane;
-  // phase of chunk c: its distance from g0 (below 2^17) modulo R
-  uint32_t ph = mod_small(((c << 4) - (uint32_t)(g0 - ga)), R, rmag);
-  for (; c < c1; c += 32u) {
-    st_out16(out + ga + ((unsigned long long)c << 4), t16[ph]);
-    ph += step512;
-    if (ph >= R) ph -= R;
+  // phase of chunk c: its distance from g0, plus the phase ph0 < R at g0, modulo R
+  uint32_t ph = mod_small(((c << 4) - (uint32_t)(g0 - ga)) + ph0, R, rmag);
+  if (step512 == 0u) {  // every chunk of this lane has the same phase
+    const uint4 v = t16[ph];
+    for (; c < c1; c += 32u) st_out16(out + ga + ((unsigned long long)c << 4), v);
+  } else {
+    for (; c < c1; c += 32u) {
+      st_out16(out + ga + ((unsigned long long)c << 4), t16[ph]);
+      ph += step512;
+      if (ph >= R) ph -= R;
+    }
   }
   unsigned long long b;
   bool ok;
@@ -1918,7 +1928,7 @@ __device__ __forceinline__ void warp_emit_replace(uint8_t* out, const uint4* t16
     b = g0 + lane;
     ok = b < gend;
   }
-  if (ok) out[b] = rs[mod_small((uint32_t)(b - g0), R, rmag)];
+  if (ok) out[b] = rs[mod_small((uint32_t)(b - g0) + ph0, R, rmag)];
 }
 
 // Input length, output range and super-tile count of the job described by p.
@@ -2002,6 +2012,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ uint32_t s_q[2];               // the super-tile this CTA works on
   __shared__ unsigned long long s_kexcl;
   __shared__ uint32_t s_cin;
+  __shared__ uint32_t s_tcnt, s_cout;       // kept starts in the super-tile looked back for; its carry-out
   __shared__ uint32_t s_fail;
   __shared__ uint32_t s_cutlen;             // exact output length of the warp region cut at n
   // per-super-tile tables, two sets: one super-tile's pass A runs while the previous one
@@ -2012,7 +2023,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ unsigned long long s_frcnt[2];          // kModeFree: super-tile function (count, local carry-out)
   __shared__ long long s_frlco[2];
   __shared__ uint32_t s_supc[2][32], s_supx[2][32];  // kModeSmall: super-tile table over carries
-  __shared__ uint32_t s_noin[2];  // pass B of the super-tile reads no input (its loads are not queued)
+  __shared__ uint32_t s_noin[2];  // pass B mode: 0 general, 1 table-driven without input, 2 table-driven
   __shared__ uint32_t s_phq[LoadRing::kPhases];
 
   const ReplaceParams& p = SEG ? s_job : pk;
@@ -2155,10 +2166,11 @@ __global__ void __launch_bounds__(kThreads, 3)
     unsigned long long fr_cnt = 0;  // kModeFree: lane 0 of warp 1
     long long fr_lco = 0;
     uint32_t sup_cnt = 0, sup_carry = lane;  // kModeSmall: warp 1, lane = carry-in
-    // Pass B reads no input when, in every warp region of a whole super-tile, the kept matches
-    // cover every byte (its output is a run of replacements, or nothing when R = 0): then the
-    // tables alone place and write the output, and the super-tile's second loads, their waits
-    // and its per-sub-tile barriers are skipped. Free mode checks
+    // Pass B of a whole super-tile is table-driven when every warp region's output is a run of
+    // replacements (the kept matches cover every byte; nothing when R = 0) or a copy of its
+    // input (no kept start): the tables alone place every region. With no copies (mode 1) pass B
+    // reads no input: the super-tile's second loads, their waits and its per-sub-tile barriers
+    // are skipped; with copies (mode 2) the loads stay. Free mode checks
     // the carry 0 (full cover of the first region needs a match at byte 0, so no match
     // of the previous super-tile can reach into it), small mode every carry into every region.
     const bool whole = !SEG && m == nsub && nsub * kWarps <= 32u && tstart + S <= n && L <= 64u &&
@@ -2168,7 +2180,8 @@ __global__ void __launch_bounds__(kThreads, 3)
       if (warp == 1) {
         // lane r stands for warp region r % 8 of sub-tile j0 + r / 8 (groups of 8 lanes)
         const uint32_t wr = lane & 7u;
-        bool ok = whole;  // whole: m <= 4, one round
+        bool ok = whole;   // every region covered end to end (whole: m <= 4, one round)
+        bool tin = whole;  // every region covered end to end or free of kept starts
         uint32_t cnt_sum = 0;
         long long lco_max = LLONG_MIN;
         for (uint32_t j0 = 0; j0 < m; j0 += 4u) {
@@ -2201,7 +2214,9 @@ __global__ void __launch_bounds__(kThreads, 3)
             uint32_t wcov = covs > wlo ? covs - wlo : 0u;
             wcov = wcov < 2048u ? wcov : 2048u;
             const uint32_t over = ce > wlo + 2048u ? ce - (wlo + 2048u) : 0u;
-            ok = __all_sync(0xffffffffu, !act || 2048u - wcov - wc * L + over == 0u);
+            const bool full = 2048u - wcov - wc * L + over == 0u;
+            ok = __all_sync(0xffffffffu, !act || full);
+            tin = __all_sync(0xffffffffu, !act || full || wc == 0u);
           }
         }
 #pragma unroll
@@ -2211,20 +2226,21 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         fr_cnt = cnt_sum;
         fr_lco = lco_max;
-        noin = ok ? 1u : 0u;
+        noin = ok ? 1u : (tin ? 2u : 0u);
         if (lane == 0 && t > 0)
           rec_store(p.rec, t, rec_word(tag, kStAgg, fr_cnt), rec_word(tag, kStAgg, (unsigned long long)fr_lco));
       }
     } else if (warp == 1) {
       const uint32_t* wt = reinterpret_cast<const uint32_t*>(wtab_b);
-      bool bad = false;  // some region is not covered from some carry
+      bool bad = false;    // some region is not covered from some carry
+      bool mixed = false;  // some region is neither covered nor free of kept starts
       if (use_rec && m <= 4u) {
         if (L == 2u)
-          fold_small_rec<2>(wt, wrec_b, subrec_b, m, whole, &bad, &sup_cnt, &sup_carry);
+          fold_small_rec<2>(wt, wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
         else if (L == 3u)
-          fold_small_rec<3>(wt, wrec_b, subrec_b, m, whole, &bad, &sup_cnt, &sup_carry);
+          fold_small_rec<3>(wt, wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
         else
-          fold_small_rec<4>(wt, wrec_b, subrec_b, m, whole, &bad, &sup_cnt, &sup_carry);
+          fold_small_rec<4>(wt, wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
       } else
       for (uint32_t j = 0; j < m; ++j) {
         uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
@@ -2242,7 +2258,10 @@ __global__ void __launch_bounds__(kThreads, 3)
           for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
             const uint32_t v = wt[(j * kWarps + w) * L + lane];  // region w from carry `lane`
             const uint32_t wc = v & 0xFFFFu, co = v >> 16;
-            if (2048u - lane - wc * L + co != 0u) bad = true;
+            if (2048u - lane - wc * L + co != 0u) {
+              bad = true;
+              if (wc != 0u) mixed = true;
+            }
           }
         }
         const uint32_t tc = __shfl_sync(0xffffffffu, cnt, sup_carry);
@@ -2250,7 +2269,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         sup_cnt += tc;
         sup_carry = tx;
       }
-      noin = (whole && !__any_sync(0xffffffffu, bad)) ? 1u : 0u;
+      noin = !whole ? 0u : (!__any_sync(0xffffffffu, bad) ? 1u : (!__any_sync(0xffffffffu, mixed) ? 2u : 0u));
       if (use_rec) {
         unsigned long long e = lane < L ? ((unsigned long long)sup_cnt | ((unsigned long long)sup_carry << 17)) : 0ull;
         const unsigned long long e1 = __shfl_sync(0xffffffffu, e, 1), e2 = __shfl_sync(0xffffffffu, e, 2),
@@ -2288,7 +2307,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     const uint32_t nx = c < NT ? c : kNone;
     s_q[0] = nx;
     if (nx != kNone) ring.push(nx, 0);
-    if (!s_noin[cset]) ring.push(tcur, 1);
+    if (s_noin[cset] != 1u) ring.push(tcur, 1);
     ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
   };
 
@@ -2352,11 +2371,14 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         s_kexcl = K;
         s_cin = c;
+        s_tcnt = (uint32_t)(Kin - K);
+        s_cout = cout;
       }
     }
     __syncthreads();
     if (tid == 0 && tnext != kNone) schedule(tnext, nset);
-    const bool noin = s_noin[set] != 0u;
+    const uint32_t pbm = s_noin[set];  // pass B mode
+    const bool noin = pbm == 1u;
     const uint32_t cin = s_cin;
     const unsigned long long kexcl = s_kexcl;
     const long long delta = (long long)R - (long long)L;
@@ -2366,12 +2388,34 @@ __global__ void __launch_bounds__(kThreads, 3)
                                                              (long long)kexcl * delta);
     const bool failed = s_fail != 0;
 
-    // ================= pass B, no input: every warp region of this whole super-tile is a run of
-    // replacements or empty. Lane r stands for region r % 8 of sub-tile r / 8: its output length
-    // from the tables, a scan over the 32 lanes places it, and each warp writes its region of
-    // every sub-tile. The last kept start follows from the regions (kept starts x0, x0 + L, ...).
+    // ================= pass B, table-driven: every warp region of this whole super-tile is a run of
+    // replacements, empty, or (mode 2) a copy of its input. Mode 2: lane r stands for region
+    // r % 8 of sub-tile r / 8: its output length from the tables, a scan over the 32 lanes
+    // places it, and each warp writes its region of every sub-tile. The last kept start follows
+    // from the regions (kept starts x0, x0 + L, ...).
     uint32_t noin_last1 = 0;
     if (noin) {
+      // every region is a run of replacements: the super-tile's output is the replacement
+      // repeated s_tcnt times from O, written in eight slices cut at 16-byte boundaries; its
+      // last match ends s_cout bytes past the super-tile
+      const uint32_t cnt = s_tcnt;
+      const uint32_t total = cnt * R;
+      noin_last1 = cnt ? m * (uint32_t)kTile + s_cout - L + 1u : 0u;
+      const bool fits_t = (O + total <= p.out_cap) && (O <= p.out_cap);
+      if (!fits_t && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
+      if (fits_t && !failed && total) {
+        const unsigned long long end = O + total;
+        const unsigned long long s0 =
+            warp == 0 ? O : (O + (((unsigned long long)total * warp) >> 3)) & ~15ull;
+        const unsigned long long s1 =
+            warp == kWarps - 1 ? end : (O + (((unsigned long long)total * (warp + 1u)) >> 3)) & ~15ull;
+        const unsigned long long a = s0 > O ? s0 : O, b = s1 < end ? s1 : end;
+        if (b > a)
+          warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, rmag, a,
+                            (uint32_t)(b - a), mod_small((uint32_t)(a - O), R, rmag));
+      }
+      O += total;
+    } else if (pbm == 2u) {
       const uint32_t jr = lane >> 3, wr = lane & 7u;
       uint32_t wc = 0, x0 = 0, olen_r = 0, we = 0;
       if (MODE == kModeFree && jr < m) {
@@ -2418,21 +2462,29 @@ __global__ void __launch_bounds__(kThreads, 3)
       const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
       const uint32_t offr = incl - olen_r;
       noin_last1 = __reduce_max_sync(0xffffffffu, wc ? jr * (uint32_t)kTile + wr * 2048u + x0 + (wc - 1u) * L + 1u : 0u);
-      const bool lit = __any_sync(0xffffffffu, olen_r != wc * R);  // a literal byte: not shown by the fold
+      // a region not shown by the fold: literal bytes beside kept matches
+      const bool odd = __any_sync(0xffffffffu, olen_r != wc * R && wc != 0u);
       const bool fits_t = (O + total <= p.out_cap) && (O <= p.out_cap);
-      if (!fits_t) {
-        if (tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
-      } else if (lit) {
-        if (tid == 0) set_error(p);
-      } else if (!failed) {
-        for (uint32_t j = 0; j < m; ++j) {
-          const uint32_t r = j * kWarps + warp;
-          const uint32_t ol = __shfl_sync(0xffffffffu, olen_r, r);
-          const uint32_t of = __shfl_sync(0xffffffffu, offr, r);
-          if (ol)
+      if (!fits_t && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
+      if (odd && tid == 0) set_error(p);
+      const bool write = fits_t && !odd && !failed;
+      for (uint32_t j = 0; j < m; ++j) {
+        const uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
+        const uint32_t r = j * kWarps + warp;
+        const uint32_t ol = __shfl_sync(0xffffffffu, olen_r, r);
+        const uint32_t of = __shfl_sync(0xffffffffu, offr, r);
+        const uint32_t cr = __shfl_sync(0xffffffffu, wc, r);
+        const uint32_t xr = __shfl_sync(0xffffffffu, x0, r);
+        if (write && ol) {
+          if (cr == 0u)
+            warp_emit_literal(p.out, tb, O + of, ol, warp * 2048u + xr);
+          else
             warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, rmag,
                               O + of, ol);
         }
+        __syncthreads();
+        ring.release();
+        if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
       }
       O += total;
     }
@@ -2440,7 +2492,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     // ================= pass B: exact kept starts and output, one warp region at a time
     uint32_t csub = cin;      // kModeFree: carry into sub-tile j
     long long last_abs = -1;  // last kept start seen by this thread
-    for (uint32_t j = 0; j < (noin ? 0u : m); ++j) {
+    for (uint32_t j = 0; j < (pbm != 0u ? 0u : m); ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
       const unsigned long long gseg = sstart + sb;
@@ -2749,8 +2801,8 @@ __global__ void __launch_bounds__(kThreads, 3)
     // ================= per-super-tile records: last kept start, totals
     {
       const uint32_t last1 = last_abs >= 0 ? (uint32_t)((unsigned long long)last_abs - tstart + 1) : 0u;
-      uint32_t tot_last1 = noin_last1;  // no input: the same in every thread already
-      if (!noin) (void)block_excl_scan1(last1, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot_last1);
+      uint32_t tot_last1 = noin_last1;  // table-driven: the same in every thread already
+      if (pbm == 0u) (void)block_excl_scan1(last1, 0u, OpMax(), s_scan2[nscan++ & 1u], &tot_last1);
       if (tid == 0) {
         const long long lastt = tot_last1 ? (long long)(tstart + tot_last1 - 1) : -1ll;
         __stcg(p.tile_last + t, lastt);

@@ -109,6 +109,21 @@ def test_runs_with_sparse_breaks(cr_lib):
                 assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (base, pat, rep)
 
 
+def test_region_blocks_copy_or_replace(cr_lib):
+    """Inputs made of 2 KiB blocks (one warp region each) that are runs of the pattern's byte,
+    of another byte, or random: whole super-tiles whose regions are each a copy or a run of
+    replacements take the table-driven pass B, the others the general one."""
+    rng = random.Random(91)
+    blocks = []
+    for _ in range(1500):
+        k = rng.random()
+        blocks.append(b"a" * 2048 if k < 0.45 else (b"b" * 2048 if k < 0.9 else rng.randbytes(2048)))
+    src = b"".join(blocks) + b"aaab"
+    for pat, rep in ((b"a", b"XY"), (b"a", b""), (b"aa", b"Q"), (b"aaa", b""), (b"b", b"cd"), (b"ab", b"Z"),
+                     (b"aab", b"0123")):
+        assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (pat, rep)
+
+
 def test_tile_boundary_straddles(cr_lib):
     rng = random.Random(5)
     for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
