@@ -1158,12 +1158,36 @@ __device__ __forceinline__ uint64_t candidates_filtered(const uint32_t w[17], co
 // lanes starts at another of its four 16-byte chunks; the first-byte mask is built in that
 // rotated order and rotated back (a 64-bit rotate). Only the rare dense branch reads the
 // segment in order.
-__device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t p4, uint32_t m4, uint32_t L) {
+// try_run (the pattern's first min(L, 4) bytes all equal its first byte b0): first test, one OR
+// per word, whether the warp's whole 2 KiB region is the byte b0 repeated (*uniform). Then
+// every window starting in the region matches those bytes, except the last lane's final
+// min(L, 4) - 1 positions, which also need the bytes after the region.
+__device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t p4, uint32_t m4, uint32_t L,
+                                                   bool try_run, bool* uniform) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t rot = (lane >> 1) & 3u;
   const uint4* v = reinterpret_cast<const uint4*>(seg);
   const uint4 q0 = v[rot], q1 = v[(rot + 1u) & 3u], q2 = v[(rot + 2u) & 3u], q3 = v[(rot + 3u) & 3u];
   const uint32_t b0 = p4 & 0xFFu, rep = b0 * 0x01010101u;
+  *uniform = false;
+  if (try_run) {
+    const uint32_t d = ((q0.x ^ rep) | (q0.y ^ rep) | (q0.z ^ rep) | (q0.w ^ rep)) |
+                       ((q1.x ^ rep) | (q1.y ^ rep) | (q1.z ^ rep) | (q1.w ^ rep)) |
+                       ((q2.x ^ rep) | (q2.y ^ rep) | (q2.z ^ rep) | (q2.w ^ rep)) |
+                       ((q3.x ^ rep) | (q3.y ^ rep) | (q3.z ^ rep) | (q3.w ^ rep));
+    if (__all_sync(0xffffffffu, d == 0u)) {
+      *uniform = true;
+      uint64_t mask = ~0ull;
+      const uint32_t lp = L < 4u ? L : 4u;
+      if (lane == 31u && lp > 1u) {
+        // leading bytes b0 of the 4 bytes after the region (the next region's, or the halo)
+        const uint32_t z = (uint32_t)__ffs(~eq_nibble(*reinterpret_cast<const uint32_t*>(seg + 64), rep) & 0x1Fu) - 1u;
+        for (uint32_t k = 1; k < lp; ++k)  // position 64 - k needs lp - k following bytes
+          if (lp - k > z) mask &= ~(1ull << (64u - k));
+      }
+      return mask;
+    }
+  }
   const uint32_t lo = eq_nibble(q0.x, rep) | (eq_nibble(q0.y, rep) << 4) | (eq_nibble(q0.z, rep) << 8) |
                       (eq_nibble(q0.w, rep) << 12) | (eq_nibble(q1.x, rep) << 16) | (eq_nibble(q1.y, rep) << 20) |
                       (eq_nibble(q1.z, rep) << 24) | (eq_nibble(q1.w, rep) << 28);
@@ -2055,6 +2079,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   uint32_t L = 0, R = 0, NT = 0, carry0 = 0, want_a = 0, step4 = 0, step512 = 0, rmag = 0;
   unsigned long long n_all = 0, n = 0, n16 = 0;
   bool rep_table = false;
+  bool run_pat = false;  // the pattern's first min(L, 4) bytes are its first byte repeated
   auto setup_job = [&]() {
     const JobDims d = job_dims(p, S);
     n_all = d.n_all;
@@ -2066,6 +2091,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     L = p.L;
     R = p.R;
     rep_table = R >= 1u && R <= 64u;
+    run_pat = ((p.p4 ^ ((p.p4 & 0xFFu) * 0x01010101u)) & p.m4) == 0u;
     step4 = R ? 4u % R : 0u;
     step512 = R ? 512u % R : 0u;
     rmag = mod_magic(R);
@@ -2107,10 +2133,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     uint8_t* const wrec_b = smem + lay.wrec + set * lay.wrec_set;
     uint8_t* const subrec_b = smem + lay.subrec + set * lay.subrec_set;
     // ================= pass A: candidates and per-warp functions of every sub-tile
+    bool run_try = run_pat;  // re-armed for every super-tile
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
-      uint64_t mask = candidates_seg(tb + sb, p.p4, p.m4, L);
+      bool uni;
+      uint64_t mask = candidates_seg(tb + sb, p.p4, p.m4, L, run_try, &uni);
+      run_try = uni;  // keep testing while the text is runs of b0
       // bounds: candidates p in [block_before, lim); a sub-tile inside both needs no masking
       const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
       const unsigned long long sub0 = tstart + (unsigned long long)j * kTile;

@@ -124,6 +124,20 @@ def test_region_blocks_copy_or_replace(cr_lib):
         assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (pat, rep)
 
 
+def test_runs_ending_near_region_edges(cr_lib):
+    """Runs of one byte that end 0-4 bytes past a 2 KiB warp region, or just before one: the
+    windows that start at the end of a uniform region reach into the next one."""
+    rng = random.Random(17)
+    parts = []
+    for _ in range(600):
+        k = rng.randrange(1, 4)
+        parts.append(b"a" * (2048 * k + rng.choice((-3, -2, -1, 0, 1, 2, 3, 4))) + rng.choice((b"b", b"ab", b"ba", b"c")))
+    src = b"".join(parts)
+    for pat, rep in ((b"a", b"XY"), (b"aa", b"Q"), (b"aaa", b""), (b"aaaa", b"Z"), (b"aaaaa", b"12"),
+                     (b"a" * 9, b""), (b"aab", b"R"), (b"aaab", b"")):
+        assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (pat, rep)
+
+
 def test_tile_boundary_straddles(cr_lib):
     rng = random.Random(5)
     for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
