@@ -2134,16 +2134,17 @@ __global__ void __launch_bounds__(kThreads, 3)
     uint8_t* const subrec_b = smem + lay.subrec + set * lay.subrec_set;
     // ================= pass A: candidates and per-warp functions of every sub-tile
     bool run_try = run_pat;  // re-armed for every super-tile
+    // bounds: candidates p in [block_before, lim); a super-tile inside both needs no masking
+    const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
+    const bool edge = tstart < p.block_before || tstart + (unsigned long long)m * kTile > lim;
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
       bool uni;
       uint64_t mask = candidates_seg(tb + sb, p.p4, p.m4, L, run_try, &uni);
       run_try = uni;  // keep testing while the text is runs of b0
-      // bounds: candidates p in [block_before, lim); a sub-tile inside both needs no masking
-      const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
       const unsigned long long sub0 = tstart + (unsigned long long)j * kTile;
-      if (sub0 < p.block_before || sub0 + kTile > lim) {
+      if (edge && (sub0 < p.block_before || sub0 + kTile > lim)) {
         uint32_t lo = 0, hi = 0;
         if (p.block_before > gseg) {
           const unsigned long long d = p.block_before - gseg;
