@@ -1819,55 +1819,43 @@ __device__ __forceinline__ uint32_t subs_in_tile(uint32_t tile, unsigned long lo
 
 // Ring of kNBuf shared-memory buffers fed by 1-D TMA loads. Every thread keeps the same
 // `consumed` count; only thread 0 issues (and tracks the issue position).
-// One queued pass over a super-tile: its first sub-tile's address, its sub-tile count, the
-// bytes of each load and of the last one, and the pass (0: A, sub-tiles with their halo; 1: B).
-struct LoadPhase {
-  const uint8_t* src;
-  uint32_t m, bytes, last, kind;
-};
-
 struct LoadRing {
   uint32_t issued, consumed;
-  uint32_t ij;      // next sub-tile of the head phase
-  uint32_t qh;      // head of the phase queue
-  uint32_t nph;     // phases queued (at most kPhases)
-  LoadPhase* q;     // the queue in shared memory
+  uint32_t ij;   // next sub-tile of the head phase
+  uint32_t qh;   // head of the phase queue
+  uint32_t nph;  // phases queued (at most kPhases)
+  uint32_t* q;   // the queue in shared memory: super-tile << 1 | kind (0: pass A, 1: pass B)
   static constexpr uint32_t kPhases = 4;
 
-  __device__ __forceinline__ void init(LoadPhase* qs) {
+  __device__ __forceinline__ void init(uint32_t* qs) {
     issued = consumed = 0;
     ij = qh = nph = 0;
     q = qs;
   }
   // Thread 0: queue the loads of one pass over super-tile t (kind 0: sub-tiles with their
-  // halo, want_a bytes, for pass A; kind 1: sub-tiles, for pass B), consumed in the order
-  // queued. The job's dimensions are resolved here, once per pass, so issuing a load is short.
-  __device__ __forceinline__ void push(uint32_t t, uint32_t kind, const ReplaceParams& p, unsigned long long S,
-                                       unsigned long long n, unsigned long long n16, uint32_t want_a, uint32_t nsub) {
-    LoadPhase& ph = q[(qh + nph) & (kPhases - 1u)];
-    const uint32_t m = subs_in_tile(t, S, n, nsub);
-    const unsigned long long start = (unsigned long long)t * S;
-    const uint32_t want = kind == 0 ? want_a : (uint32_t)kTile;
-    const unsigned long long avail = n16 - (start + (unsigned long long)(m - 1u) * kTile);
-    ph.src = p.in + start;
-    ph.m = m;
-    ph.bytes = want;
-    ph.last = avail < want ? (uint32_t)avail : want;
-    ph.kind = kind;
+  // halo, for pass A; kind 1: sub-tiles, for pass B), consumed in the order queued.
+  __device__ __forceinline__ void push(uint32_t t, uint32_t kind) {
+    q[(qh + nph) & (kPhases - 1u)] = (t << 1) | kind;
     ++nph;
   }
   // Thread 0: keep up to kNBuf loads in flight.
-  __device__ __forceinline__ void issue(uint8_t* smem, const LayoutS& lay, uint64_t* bars) {
+  __device__ __forceinline__ void issue(const ReplaceParams& p, uint8_t* smem, const LayoutS& lay, uint64_t* bars,
+                                        unsigned long long S, unsigned long long n16, uint32_t want_a,
+                                        unsigned long long n, uint32_t nsub) {
     while (issued - consumed < (uint32_t)kNBuf && nph > 0) {
-      const LoadPhase& ph = q[qh];
-      const uint32_t m = ph.m;
-      const uint32_t bytes = ij + 1u == m ? ph.last : ph.bytes;
+      const uint32_t e = q[qh];
+      const uint32_t t = e >> 1, kind = e & 1u;
+      const uint32_t m = subs_in_tile(t, S, n, nsub);
+      const unsigned long long start = (unsigned long long)t * S + (unsigned long long)ij * kTile;
+      const unsigned long long avail = n16 - start;
+      const uint32_t want = kind == 0 ? want_a : (uint32_t)kTile;
+      const uint32_t bytes = avail < want ? (uint32_t)avail : want;
       const uint32_t b = issued % kNBuf;
       // no proxy fence: the buffer's earlier contents were only read, and every read of them
       // completed before the block barrier that freed it (a write cannot reach a finished read)
       mbar_arrive_expect_tx(&bars[b], bytes);
-      bulk_load_hint(smem + lay.in0 + b * lay.inbytes, ph.src + (size_t)ij * kTile, bytes, &bars[b],
-                     ph.kind == 0 ? l2_policy_evict_last() : l2_policy_evict_first());
+      bulk_load_hint(smem + lay.in0 + b * lay.inbytes, p.in + start, bytes, &bars[b],
+                     kind == 0 ? l2_policy_evict_last() : l2_policy_evict_first());
       ++issued;
       if (++ij == m) {
         ij = 0;
@@ -2061,7 +2049,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ long long s_frlco[2];
   __shared__ uint32_t s_supc[2][32], s_supx[2][32];  // kModeSmall: super-tile table over carries
   __shared__ uint32_t s_noin[2];  // pass B mode: 0 general, 1 table-driven without input, 2 table-driven
-  __shared__ LoadPhase s_phq[LoadRing::kPhases];
+  __shared__ uint32_t s_phq[LoadRing::kPhases];
 
   const ReplaceParams& p = SEG ? s_job : pk;
   unsigned int* const sched = SEG ? sl.sched : &pk.res->tile_counter;  // claim counter, then finished CTAs
@@ -2199,7 +2187,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       __syncthreads();
       ring.release();
-      if (tid == 0) ring.issue(smem, lay, s_bar);
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
     }
 
     // ================= fold the sub-tiles into the super-tile function
@@ -2349,9 +2337,9 @@ __global__ void __launch_bounds__(kThreads, 3)
     const uint32_t c = atomicAdd(sched, 1u);
     const uint32_t nx = c < NT ? c : kNone;
     s_q[0] = nx;
-    if (nx != kNone) ring.push(nx, 0, p, S, n, n16, want_a, nsub);
-    if (s_noin[cset] != 1u) ring.push(tcur, 1, p, S, n, n16, want_a, nsub);
-    ring.issue(smem, lay, s_bar);
+    if (nx != kNone) ring.push(nx, 0);
+    if (s_noin[cset] != 1u) ring.push(tcur, 1);
+    ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
   };
 
   // look-back, pass B and records of super-tile t, whose pass A filled set `set`; after the
@@ -2527,7 +2515,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         __syncthreads();
         ring.release();
-        if (tid == 0) ring.issue(smem, lay, s_bar);
+        if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
       }
       O += total;
     }
@@ -2838,7 +2826,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       O += sub_total;
       __syncthreads();
       ring.release();
-      if (tid == 0) ring.issue(smem, lay, s_bar);
+      if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
     }
 
     // ================= per-super-tile records: last kept start, totals
@@ -2877,16 +2865,16 @@ __global__ void __launch_bounds__(kThreads, 3)
       s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
       if (s_q[0] != kNone) {
         const JobDims d = job_dims(p, S);
-        ring.push(s_q[0], 0, p, S, d.n, d.n16, d.want_a, nsub);
-        ring.push(s_q[0], 1, p, S, d.n, d.n16, d.want_a, nsub);
-        ring.issue(smem, lay, s_bar);
+        ring.push(s_q[0], 0);
+        ring.push(s_q[0], 1);
+        ring.issue(p, smem, lay, s_bar, S, d.n16, d.want_a, d.n, nsub);
       }
     } else {
       const uint32_t first = atomicAdd(sched, 1u);
       s_q[0] = first < NT ? first : kNone;
       if (s_q[0] != kNone) {
-        ring.push(s_q[0], 0, p, S, n, n16, want_a, nsub);
-        ring.issue(smem, lay, s_bar);
+        ring.push(s_q[0], 0);
+        ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
       }
     }
   }
@@ -2912,9 +2900,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         s_q[0] = seg_claim(sl, s_job, &s_jobid, &s_newjob);
         if (s_q[0] != kNone) {
           const JobDims d = job_dims(p, S);
-          ring.push(s_q[0], 0, p, S, d.n, d.n16, d.want_a, nsub);
-          ring.push(s_q[0], 1, p, S, d.n, d.n16, d.want_a, nsub);
-          ring.issue(smem, lay, s_bar);
+          ring.push(s_q[0], 0);
+          ring.push(s_q[0], 1);
+          ring.issue(p, smem, lay, s_bar, S, d.n16, d.want_a, d.n, nsub);
         }
       }
     }
