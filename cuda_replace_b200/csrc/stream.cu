@@ -344,8 +344,14 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
     if (e != cudaSuccess) return (int)e;
   }
 
-  // the result: page-locked, from the pool; grows by half when a chunk does not fit
+  // the result: page-locked, from the pool; grows by half when a chunk does not fit. One pair:
+  // sized for the most matches it can keep (n / L of them), up to four times the input.
   size_t ocap = n + n / 8 + (64u << 20), written = 0;
+  if (count == 1) {
+    const size_t L = (size_t)pat_lens[0], R = (size_t)rep_lens[0];
+    const size_t bound = R > L ? n + (n / L) * (R - L) : n;
+    ocap = std::min(bound, 4 * n + (64u << 20)) + 64;
+  }
   uint8_t* hout = static_cast<uint8_t*>(pool.get(ocap, &e));
   if (!hout) return (int)e;
 

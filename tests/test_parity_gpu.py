@@ -138,6 +138,30 @@ def test_runs_ending_near_region_edges(cr_lib):
         assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (pat, rep)
 
 
+def test_large_inputs_unified_and_stream(cr_lib):
+    """Inputs above 256 MiB through unified() and through the native chunk-major stream with
+    one pair (chunks of n/8): results equal bytes.replace, also for matches planted across every
+    chunk join, with expansion (the stream sizes its result for n/L matches), deletion and a
+    bordered pattern."""
+    n = (256 << 20) + 12345
+    chunk = max(32 << 20, ((n // 8 + (1 << 20) - 1) >> 20) << 20)
+    rng = random.Random(23)
+    text = bytearray(rng.randbytes(1 << 20) * (n // (1 << 20) + 1))[:n]
+    for c in range(chunk, n, chunk):  # a match straddling every join
+        text[c - 2:c + 3] = b"&amp;"
+        text[c - 7:c - 4] = b"aab"
+    text = bytes(text)
+    for pat, rep in ((b"&amp;", b"&"), (b"&amp;", b"<entity>"), (b"aab", b""), (b"\x00", b"0123")):
+        want = text.replace(pat, rep)
+        assert cr_lib.unified(text, pat, rep) == want, (pat, rep)
+        assert _native_stream(cr_lib, text, [(pat, rep)], chunk) == want, (pat, rep)
+    run = b"a" * n
+    for pat, rep in ((b"aa", b"X"), (b"a", b"bcd")):
+        want = run.replace(pat, rep)
+        assert cr_lib.unified(run, pat, rep) == want, (pat, rep)
+        assert _native_stream(cr_lib, run, [(pat, rep)], chunk) == want, (pat, rep)
+
+
 def test_tile_boundary_straddles(cr_lib):
     rng = random.Random(5)
     for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
