@@ -80,6 +80,12 @@ void host_free(void* p) {
 
 #define CR_EXPORT extern "C" __attribute__((visibility("default")))
 
+// unified() takes its chunked path (uploads, replaces and downloads of successive chunks
+// overlapped) for page-locked inputs from kUnifiedChunkedMin bytes, in at most kUnifiedChunks
+// chunks of at least 32 MiB.
+constexpr size_t kUnifiedChunkedMin = (size_t)256 << 20;
+constexpr int kUnifiedChunks = 8;
+
 namespace {
 
 using crb::ApplyResult;
@@ -137,6 +143,12 @@ struct Session {
   int q_kind = 0;
   unsigned long long q_n = 0;
   ReplaceParams q_params;
+
+  // unified() on a large page-locked input: upload and download streams, one event per chunk
+  cudaStream_t up = nullptr, down = nullptr;
+  cudaEvent_t ev_up[kUnifiedChunks] = {}, ev_done[kUnifiedChunks] = {};
+  unsigned int* carry2 = nullptr;           // device: carry into / out of the current chunk
+  unsigned long long* olen_dev = nullptr;   // device: output end of the current chunk
 };
 
 cudaError_t dev_grow(uint8_t** ptr, size_t* cap, size_t need, bool keep, size_t keep_len, cudaStream_t st) {
@@ -253,6 +265,20 @@ void session_free(Session* s) {
   if (s->ext_host) cudaFreeHost(s->ext_host);
   if (s->lens) cudaFree(s->lens);
   if (s->lens_host) cudaFreeHost(s->lens_host);
+  for (int k = 0; k < kUnifiedChunks; ++k) {
+    if (s->ev_up[k]) cudaEventDestroy(s->ev_up[k]);
+    if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
+  }
+  if (s->up) {
+    cudaStreamSynchronize(s->up);
+    cudaStreamDestroy(s->up);
+  }
+  if (s->down) {
+    cudaStreamSynchronize(s->down);
+    cudaStreamDestroy(s->down);
+  }
+  if (s->carry2) cudaFree(s->carry2);
+  if (s->olen_dev) cudaFree(s->olen_dev);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -901,6 +927,125 @@ CR_EXPORT void cuda_replace_close(void* h) {
   session_free(s);
 }
 
+// unified() for a large page-locked input and a pattern the super-tile kernel takes: every
+// chunk's upload is queued at once; each chunk is replaced as soon as it is on the device (its
+// last L - 1 bytes held back for the next chunk, the coverage carried across on the device)
+// into the session's output buffer, and its output is downloaded into the result while the
+// next chunks upload. Returns 1 when the call does not qualify (the caller takes the
+// single-launch path), else 0 or an error.
+int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat, uint32_t L, const uint8_t* rep,
+                    uint32_t R, uint8_t** out_host, size_t* out_len) {
+  if (n < kUnifiedChunkedMin || L == 0 || L > (uint32_t)crb::kInlineMax || R > (uint32_t)crb::kInlineMax ||
+      !host_is_pinned(src))
+    return 1;
+  ReplaceParams proto;
+  memset(&proto, 0, sizeof(proto));
+  crb::prepare_pattern_fields(proto, pat, L);
+  proto.R = R;
+  proto.nsub = crb::super_nsub(proto.mode, L);
+  if (!proto.nsub) return 1;
+  const size_t bound = output_bound(n, L, R);
+  if (bound > 4 * n + ((size_t)64 << 20)) return 1;  // a large expansion: the single-launch path sizes it
+  memcpy(proto.pat, pat, L);
+  if (R) memcpy(proto.rep, rep, R);
+  const size_t P = L - 1;  // bytes held back at the end of every chunk but the last
+  const size_t chunk = std::max<size_t>((size_t)32 << 20, round_up((n + kUnifiedChunks - 1) / kUnifiedChunks, 1u << 20));
+  // Chunk k uploads input [bnd(k), bnd(k + 1)) with bnd(k) = k * chunk + P for 0 < k: its
+  // replace then starts P bytes earlier, at k * chunk, a 16-byte boundary as the loads need.
+  size_t nchunks = (n + chunk - 1) / chunk;
+  while (nchunks > 1 && (nchunks - 1) * chunk + P >= n) --nchunks;
+  if (nchunks > (size_t)kUnifiedChunks) return 1;
+  auto bnd = [&](size_t k) -> size_t { return k == 0 ? 0 : (k >= nchunks ? n : k * chunk + P); };
+  const size_t tile_bytes = (size_t)crb::kTile * proto.nsub;
+
+  cudaError_t e = cudaSuccess;
+  if (!s->up) e = cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !s->down) e = cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking);
+  for (int k = 0; k < kUnifiedChunks && e == cudaSuccess; ++k) {
+    if (!s->ev_up[k]) e = cudaEventCreateWithFlags(&s->ev_up[k], cudaEventDisableTiming);
+    if (e == cudaSuccess && !s->ev_done[k]) e = cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess && !s->carry2) e = cudaMalloc(&s->carry2, 2 * sizeof(unsigned int));
+  if (e == cudaSuccess && !s->olen_dev) e = cudaMalloc(&s->olen_dev, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = dev_grow(&s->buf, &s->buf_cap, n, false, 0, s->stream);
+  if (e == cudaSuccess) e = dev_grow(&s->alt, &s->alt_cap, bound ? bound : 1, false, 0, s->stream);
+  if (e == cudaSuccess) e = ensure_scratch(s, (2 * chunk + P + tile_bytes - 1) / tile_bytes + 1, proto.agg_entries);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->carry2, 0, 2 * sizeof(unsigned int), s->stream);
+  if (e != cudaSuccess) return (int)e;
+  uint8_t* host = static_cast<uint8_t*>(pinned_pool().get(bound ? bound : 1, &e));
+  if (!host) return (int)e;
+  for (size_t k = 0; k < nchunks && e == cudaSuccess; ++k) {
+    const size_t a = bnd(k), m = bnd(k + 1) - a;
+    e = cudaMemcpyAsync(s->buf + a, src + a, m, cudaMemcpyHostToDevice, s->up);
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev_up[k], s->up);
+  }
+  int rc = (int)e;
+  size_t O = 0;
+  for (size_t k = 0; k < nchunks && rc == 0; ++k) {
+    const size_t a = bnd(k), m = bnd(k + 1) - a;
+    const bool first = k == 0, final = k + 1 == nchunks;
+    const size_t held = first ? 0 : P;  // the previous chunk's last bytes, matched again here
+    ReplaceParams p = proto;
+    p.in = s->buf + (a - held);  // k * chunk: 16-byte aligned
+    p.n = held + m;
+    p.hold = final ? 0 : P;
+    p.carry0_dev = s->carry2 + (k & 1);
+    p.carry_out = s->carry2 + ((k & 1) ^ 1);
+    p.out = s->alt;
+    p.out_cap = s->alt_cap;
+    p.len_bias = O;
+    p.len_out = s->olen_dev;
+    p.num_tiles = (uint32_t)((p.n + tile_bytes - 1) / tile_bytes + 1);
+    p.status = s->status;
+    p.incl = s->incl;
+    p.agg = s->agg;
+    p.res = s->res;
+    p.tile_last = s->tile_last;
+    p.rec = s->rec;
+    p.epoch = next_epoch(s);
+    e = cudaStreamWaitEvent(s->stream, s->ev_up[k], 0);
+    if (e == cudaSuccess) e = crb::launch_replace_super(p, s->stream, nullptr);
+    if (e == cudaSuccess) {
+      ++s->launches;
+      e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+      rc = (int)e;
+      break;
+    }
+    const ApplyResult r = *s->res_host;
+    if (r.error_epoch == p.epoch || r.overflow_epoch == p.epoch) {
+      rc = kErrUnknown;  // a bounded wait gave up (the buffer holds the worst case: no overflow)
+      break;
+    }
+    const size_t olen = (size_t)r.out_len;
+    if (olen) {
+      e = cudaEventRecord(s->ev_done[k], s->stream);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s->down, s->ev_done[k], 0);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(host + O, s->alt + O, olen, cudaMemcpyDeviceToHost, s->down);
+      if (e != cudaSuccess) {
+        rc = (int)e;
+        break;
+      }
+    }
+    O += olen;
+  }
+  const cudaError_t e1 = cudaStreamSynchronize(s->down);
+  const cudaError_t e2 = cudaStreamSynchronize(s->up);
+  if (rc == 0 && e1 != cudaSuccess) rc = (int)e1;
+  if (rc == 0 && e2 != cudaSuccess) rc = (int)e2;
+  s->len = 0;  // the session's buffers hold no complete content now
+  s->q_kind = 0;
+  if (rc != 0 || O == 0) {
+    pinned_pool().put(host);
+    return rc;
+  }
+  *out_host = host;
+  *out_len = O;
+  return 0;
+}
+
 CR_EXPORT int cuda_replace_unified(const uint8_t* src, size_t src_len, const uint8_t* pat, int pat_len,
                                    const uint8_t* rep, int rep_len, uint8_t** out_host, size_t* out_len) {
   if (!out_host || !out_len) return -1;
@@ -914,6 +1059,20 @@ CR_EXPORT int cuda_replace_unified(const uint8_t* src, size_t src_len, const uin
   if (!s) {
     rc = session_create(&s);
     if (rc != 0) return rc;
+  }
+  if (pat_len > 0 && rep_len >= 0 && pat && (rep || rep_len == 0)) {
+    rc = unified_chunked(s, src, src_len, pat, (uint32_t)pat_len, rep, (uint32_t)rep_len, out_host, out_len);
+    if (rc != 1) {
+      if (rc == 0) {
+        cache_give(s);
+      } else {
+        session_free(s);
+        *out_host = nullptr;
+        *out_len = 0;
+      }
+      return rc;
+    }
+    rc = 0;
   }
   rc = session_load(s, src, src_len);
   if (rc == 0) rc = apply_one(s, pat, pat_len, rep, rep_len, 0, nullptr, nullptr);

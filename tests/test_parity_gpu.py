@@ -162,6 +162,47 @@ def test_large_inputs_unified_and_stream(cr_lib):
         assert _native_stream(cr_lib, run, [(pat, rep)], chunk) == want, (pat, rep)
 
 
+def test_unified_page_locked_large_chunked(cr_lib):
+    """unified() on a page-locked input of 256 MiB or more takes the chunked path (uploads,
+    replaces and downloads of up to eight chunks overlapped): results equal bytes.replace, also
+    for matches planted across every chunk join, for bordered and free patterns, expansion and
+    deletion."""
+    import ctypes as C
+
+    import torch
+
+    n = (300 << 20) + 777
+    chunk = max(32 << 20, ((n + 7) // 8 + (1 << 20) - 1) >> 20 << 20)
+    rng = random.Random(41)
+    text = bytearray(rng.randbytes(1 << 20) * (n // (1 << 20) + 1))[:n]
+    for j in range(chunk, n - chunk // 2, chunk):
+        # a chunk's replace starts at j, its upload at j + L - 1: matches straddle both joins
+        for c in (j, j + 4, j + 3, j + 1):
+            text[c - 2 + 64 * (c - j):c + 3 + 64 * (c - j)] = b"&amp;"
+        text[j - 3:j + 1] = b"abab"      # straddles the join by one byte
+        text[j + 200:j + 204] = b"abab"
+        text[j + 256 - 4:j + 256] = b"abab"
+    text = bytes(text)
+    run = b"a" * n
+    out_ptr = C.POINTER(C.c_uint8)()
+    out_len = C.c_size_t()
+    for src, cases in ((text, ((b"&amp;", b"&"), (b"&amp;", b"<e>"), (b"abab", b"X"), (b"\x00", b""))),
+                       (run, ((b"aa", b"X"), (b"a", b"bcd"), (b"aaa", b"")))):
+        h = torch.frombuffer(bytearray(src), dtype=torch.uint8).pin_memory()
+        for pat, rep in cases:
+            pb, rb = C.create_string_buffer(pat, len(pat)), C.create_string_buffer(rep, len(rep) or 1)
+            rc = cr_lib.lib.cuda_replace_unified(C.cast(h.data_ptr(), C.POINTER(C.c_uint8)), n,
+                                                 C.cast(pb, C.POINTER(C.c_uint8)), len(pat),
+                                                 C.cast(rb, C.POINTER(C.c_uint8)), len(rep),
+                                                 C.byref(out_ptr), C.byref(out_len))
+            assert rc == 0
+            got = C.string_at(out_ptr, out_len.value) if out_len.value else b""
+            if out_len.value:
+                cr_lib.lib.cuda_free_host(out_ptr)
+            assert got == src.replace(pat, rep), (pat, rep)
+        del h
+
+
 def test_tile_boundary_straddles(cr_lib):
     rng = random.Random(5)
     for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
