@@ -84,7 +84,7 @@ void host_free(void* p) {
 // overlapped) for page-locked inputs from kUnifiedChunkedMin bytes, in at most kUnifiedChunks
 // chunks of at least 32 MiB.
 constexpr size_t kUnifiedChunkedMin = (size_t)256 << 20;
-constexpr int kUnifiedChunks = 8;
+constexpr int kUnifiedChunks = 16;
 
 namespace {
 

@@ -164,7 +164,7 @@ def test_large_inputs_unified_and_stream(cr_lib):
 
 def test_unified_page_locked_large_chunked(cr_lib):
     """unified() on a page-locked input of 256 MiB or more takes the chunked path (uploads,
-    replaces and downloads of up to eight chunks overlapped): results equal bytes.replace, also
+    replaces and downloads of up to sixteen chunks overlapped): results equal bytes.replace, also
     for matches planted across every chunk join, for bordered and free patterns, expansion and
     deletion."""
     import ctypes as C
@@ -172,7 +172,7 @@ def test_unified_page_locked_large_chunked(cr_lib):
     import torch
 
     n = (300 << 20) + 777
-    chunk = max(32 << 20, ((n + 7) // 8 + (1 << 20) - 1) >> 20 << 20)
+    chunk = max(32 << 20, ((n + 15) // 16 + (1 << 20) - 1) >> 20 << 20)
     rng = random.Random(41)
     text = bytearray(rng.randbytes(1 << 20) * (n // (1 << 20) + 1))[:n]
     for j in range(chunk, n - chunk // 2, chunk):
