@@ -973,7 +973,10 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   if (e == cudaSuccess) e = cudaMemsetAsync(s->carry2, 0, 2 * sizeof(unsigned int), s->stream);
   if (e != cudaSuccess) return (int)e;
   uint8_t* host = static_cast<uint8_t*>(pinned_pool().get(bound ? bound : 1, &e));
-  if (!host) return (int)e;
+  if (!host) {
+    cudaGetLastError();  // a page-locked block of the worst case was refused: the single-launch
+    return 1;            // path allocates the result at its exact size
+  }
   for (size_t k = 0; k < nchunks && e == cudaSuccess; ++k) {
     const size_t a = bnd(k), m = bnd(k + 1) - a;
     e = cudaMemcpyAsync(s->buf + a, src + a, m, cudaMemcpyHostToDevice, s->up);
