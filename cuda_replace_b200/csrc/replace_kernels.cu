@@ -1117,47 +1117,15 @@ __device__ __forceinline__ uint32_t eq_nibble(uint32_t w, uint32_t rep) {
   return ((~nz & 0x80808080u) * 0x00204081u) >> 28;
 }
 
-// 64-bit mask of the segment's bytes equal to the byte replicated in rep.
-__device__ __forceinline__ uint64_t byte_eq_mask(const uint32_t w[17], uint32_t rep) {
-  uint32_t lo = 0, hi = 0;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    lo |= eq_nibble(w[i], rep) << (4 * i);
-    hi |= eq_nibble(w[i + 8], rep) << (4 * i);
-  }
-  return ((uint64_t)hi << 32) | lo;
-}
-
-// Candidate starts of one 64-byte segment, comparing the first min(L, 4) pattern bytes
-// (as candidates_from_words) with fewer instructions: the positions holding the first pattern
-// byte come from four bytes per operation; L = 1 needs nothing more and a doubled first byte
-// (L = 2, e.g. "aa") a shift; otherwise each such position is checked with one unaligned
-// 4-byte read, unless a lane of the warp has many of them (dense text such as a run of one
-// byte), where every window is compared.
-__device__ __forceinline__ uint64_t candidates_filtered(const uint32_t w[17], const uint8_t* seg, uint32_t p4,
-                                                        uint32_t m4, uint32_t L) {
-  const uint32_t b0 = p4 & 0xFFu;
-  const uint64_t e0 = byte_eq_mask(w, b0 * 0x01010101u);
-  if (L == 1u) return e0;
-  if (L == 2u && ((p4 >> 8) & 0xFFu) == b0) {
-    const uint64_t next = (w[16] & 0xFFu) == b0 ? 1ull : 0ull;  // byte 64: the next segment's first
-    return e0 & ((e0 >> 1) | (next << 63));
-  }
-  if (__any_sync(0xffffffffu, __popcll(e0) > 12)) return candidates_from_words(w, p4, m4);
-  uint64_t m = e0, out = 0;
-  while (m) {
-    const int b = __ffsll((long long)m) - 1;
-    m &= m - 1;
-    if (((ld_u32_unaligned(seg + b) ^ p4) & m4) == 0u) out |= 1ull << b;
-  }
-  return out;
-}
-
-// candidates_filtered for the 64-byte segment at seg (shared memory), reading it without bank
-// conflicts: lanes 64 bytes apart would hit the same banks four at a time, so each pair of
-// lanes starts at another of its four 16-byte chunks; the first-byte mask is built in that
-// rotated order and rotated back (a 64-bit rotate). Only the rare dense branch reads the
-// segment in order.
+// Candidate starts of the 64-byte segment at seg (shared memory), comparing the first min(L, 4)
+// pattern bytes (as candidates_from_words) with fewer instructions: the positions holding the
+// first pattern byte come from four bytes per operation; L = 1 needs nothing more and a
+// doubled first byte (L = 2, e.g. "aa") a shift; otherwise each such position is checked with
+// one unaligned 4-byte read, unless a lane of the warp has many of them (dense text), where
+// every window is compared. The segment is read without bank conflicts: lanes 64 bytes apart
+// would hit the same banks four at a time, so each pair of lanes starts at another of its four
+// 16-byte chunks; the first-byte mask is built in that rotated order and rotated back (a 64-bit
+// rotate). Only the rare dense branch reads the segment in order.
 // try_run (the pattern's first min(L, 4) bytes all equal its first byte b0): first test, one OR
 // per word, whether the warp's whole 2 KiB region is the byte b0 repeated (*uniform). Then
 // every window starting in the region matches those bytes, except the last lane's final
