@@ -203,6 +203,35 @@ def test_unified_page_locked_large_chunked(cr_lib):
         del h
 
 
+def test_fuzz_runs_blocks_and_text(cr_lib):
+    """Seeded inputs of 1-3 MB mixing runs of one byte (often whole 2 KiB regions), short-alphabet
+    text and random bytes, against bordered and free patterns of 1-6 bytes and replacements of
+    0-8 bytes: every pass-B mode (no input, table-driven, general) and the uniform-region test
+    meet each other at super-tile edges."""
+    pats = [b"a", b"aa", b"aaa", b"ab", b"aba", b"b", b"ba", b"abab", b"aab", b"aaaaaa", b"\x00"]
+    for seed in range(24):
+        rng = random.Random(1000 + seed)
+        parts, size = [], rng.randrange(1 << 20, 3 << 20)
+        total = 0
+        while total < size:
+            k = rng.random()
+            if k < 0.35:
+                part = rng.choice(b"ab").to_bytes(1, "little") * rng.choice((2048, 4096, rng.randrange(1, 20000)))
+            elif k < 0.7:
+                part = bytes(rng.choice(b"ab") for _ in range(rng.randrange(1, 3000)))
+            elif k < 0.85:
+                part = bytes(rng.choice(b"abc") for _ in range(rng.randrange(1, 3000)))
+            else:
+                part = rng.randbytes(rng.randrange(1, 5000))
+            parts.append(part)
+            total += len(part)
+        src = b"".join(parts)
+        for _ in range(3):
+            pat = rng.choice(pats)
+            rep = bytes(rng.choice(b"XYZ") for _ in range(rng.randrange(0, 9)))
+            assert cr_lib.unified(src, pat, rep) == src.replace(pat, rep), (seed, pat, rep)
+
+
 def test_tile_boundary_straddles(cr_lib):
     rng = random.Random(5)
     for L in (2, 3, 4, 5, 8, 16, 64, 65, 100, 300):
