@@ -1455,6 +1455,19 @@ __device__ __forceinline__ uint32_t tab4_entry(unsigned long long d0, unsigned l
   return (uint32_t)((c & 1u) ? (w >> 19) : w) & 0x7FFFFu;
 }
 
+// A warp region whose 2 KiB are all candidates (a run such as "aaaa" for "aa", L <= 4): from
+// carry-in c the greedy keeps c, c + L, c + 2L, ..., so its tables have closed forms, and pass
+// A records only that the region is dense. Region entry (kept count | carry-out << 16):
+__device__ __forceinline__ uint32_t dense_region_entry(uint32_t c, uint32_t L) {
+  const uint32_t cnt = (2048u - c + L - 1u) / L;
+  return cnt | ((c + cnt * L - 2048u) << 16);
+}
+// ... and the carry into the segment at byte `off` of the region:
+__device__ __forceinline__ uint32_t dense_seg_carry(uint32_t c, uint32_t off, uint32_t L) {
+  const uint32_t q = off > c ? (off - c + L - 1u) / L : 0u;  // kept starts before the segment
+  return c + q * L - off;
+}
+
 // Functions over carries 0..LL-1 (patterns of LL <= 4 bytes) with wide counts, one register
 // per entry: kept count in bits 0-23, carry-out in bits 24-31.
 template <int LL>
@@ -1554,9 +1567,9 @@ __device__ __forceinline__ bool lookback_small_rec(const ReplaceParams& p, uint3
 // `whole`: some region is not covered end to end from some carry (*bad), or is neither covered
 // nor free of kept starts (*mixed).
 template <int LL>
-__device__ __forceinline__ void fold_small_rec(const uint32_t* wt, uint8_t* wrec, uint8_t* subrec, uint32_t m,
-                                               bool whole, bool* bad, bool* mixed, uint32_t* sup_cnt,
-                                               uint32_t* sup_carry) {
+__device__ __forceinline__ void fold_small_rec(const uint32_t* wt, const uint8_t* dense, uint8_t* wrec,
+                                               uint8_t* subrec, uint32_t m, bool whole, bool* bad, bool* mixed,
+                                               uint32_t* sup_cnt, uint32_t* sup_carry) {
   const uint32_t lane = threadIdx.x & 31u, jr = lane >> 3, wr = lane & 7u;
   const bool act = jr < m;
   uint32_t g[4];
@@ -1564,7 +1577,7 @@ __device__ __forceinline__ void fold_small_rec(const uint32_t* wt, uint8_t* wrec
   for (uint32_t y = 0; y < (uint32_t)LL; ++y) {
     g[y] = y << 24;
     if (act) {
-      const uint32_t v = wt[lane * LL + y];
+      const uint32_t v = dense[lane] ? dense_region_entry(y, LL) : wt[lane * LL + y];
       const uint32_t wc = v & 0xFFFFu, co = v >> 16;
       g[y] = wc | (co << 24);
       if (whole && 2048u - y - wc * LL + co != 0u) {
@@ -1675,26 +1688,11 @@ __device__ __forceinline__ void ks_compose_n(uint32_t& t0, uint32_t& t1, uint32_
 // segment (carry into it for each warp carry-in) and, from lane 31, the warp function.
 template <int LL>
 __device__ __forceinline__ void ks_warp_tables(uint64_t mask, uint32_t inv_l, uint64_t stride, uint8_t* srec_row,
-                                               uint32_t* wtab_row) {
+                                               uint32_t* wtab_row, uint8_t* dense) {
   const uint32_t lane = threadIdx.x & 31u;
-  if (__all_sync(0xffffffffu, mask == ~0ull)) {
-    // every position of the warp's 2 KiB is a candidate (a run such as "aaaa" for "aa"): from
-    // carry-in c the greedy keeps c, c + L, c + 2L, ... so both tables have a closed form
-    const uint32_t off = 64u * lane;
-#pragma unroll
-    for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
-      const uint32_t q = off > c ? (off - c + LL - 1u) / LL : 0u;  // kept starts before this segment
-      srec_row[c] = (uint8_t)(c + q * LL - off);
-    }
-    if (lane == 31) {
-#pragma unroll
-      for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
-        const uint32_t cnt = (2048u - c + LL - 1u) / LL;
-        wtab_row[c] = cnt | ((c + cnt * LL - 2048u) << 16);
-      }
-    }
-    return;
-  }
+  const bool all = __all_sync(0xffffffffu, mask == ~0ull);
+  if (lane == 0) *dense = all ? 1u : 0u;
+  if (all) return;  // closed forms (dense_region_entry, dense_seg_carry): no tables
   uint32_t ent[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
   for (uint32_t c = 0; c < (uint32_t)LL; ++c) {
@@ -2016,7 +2014,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ unsigned long long s_frcnt[2];          // kModeFree: super-tile function (count, local carry-out)
   __shared__ long long s_frlco[2];
   __shared__ uint32_t s_supc[2][32], s_supx[2][32];  // kModeSmall: super-tile table over carries
-  __shared__ uint32_t s_noin[2];  // pass B mode: 0 general, 1 table-driven without input, 2 table-driven
+  __shared__ uint32_t s_noin[2];
+  __shared__ uint8_t s_dense[2][kMaxSub * kWarps];  // kModeSmall, L <= 4: region (j, w) is dense  // pass B mode: 0 general, 1 table-driven without input, 2 table-driven
   __shared__ uint32_t s_phq[LoadRing::kPhases];
 
   const ReplaceParams& p = SEG ? s_job : pk;
@@ -2127,11 +2126,11 @@ __global__ void __launch_bounds__(kThreads, 3)
         uint8_t* srec = srec_b + (size_t)j * kThreads * L;
         uint32_t* wtab = reinterpret_cast<uint32_t*>(wtab_b) + (size_t)(j * kWarps + warp) * L;
         if (L == 2u) {
-          ks_warp_tables<2>(mask, p.inv_l, p.stride_mask, srec + tid * 2u, wtab);
+          ks_warp_tables<2>(mask, p.inv_l, p.stride_mask, srec + tid * 2u, wtab, &s_dense[set][j * kWarps + warp]);
         } else if (L == 3u) {
-          ks_warp_tables<3>(mask, p.inv_l, p.stride_mask, srec + tid * 3u, wtab);
+          ks_warp_tables<3>(mask, p.inv_l, p.stride_mask, srec + tid * 3u, wtab, &s_dense[set][j * kWarps + warp]);
         } else if (L == 4u) {
-          ks_warp_tables<4>(mask, p.inv_l, p.stride_mask, srec + tid * 4u, wtab);
+          ks_warp_tables<4>(mask, p.inv_l, p.stride_mask, srec + tid * 4u, wtab, &s_dense[set][j * kWarps + warp]);
         } else {
           // segment tables in shared memory, then lanes-over-carries walks of the warp's
           // own 32 segments (only rows of this warp are read: a warp barrier suffices)
@@ -2235,11 +2234,11 @@ __global__ void __launch_bounds__(kThreads, 3)
       bool mixed = false;  // some region is neither covered nor free of kept starts
       if (use_rec && m <= 4u) {
         if (L == 2u)
-          fold_small_rec<2>(wt, wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
+          fold_small_rec<2>(wt, s_dense[set], wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
         else if (L == 3u)
-          fold_small_rec<3>(wt, wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
+          fold_small_rec<3>(wt, s_dense[set], wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
         else
-          fold_small_rec<4>(wt, wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
+          fold_small_rec<4>(wt, s_dense[set], wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
       } else
       for (uint32_t j = 0; j < m; ++j) {
         uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
@@ -2247,7 +2246,8 @@ __global__ void __launch_bounds__(kThreads, 3)
 #pragma unroll
         for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
           if (lane < L) wrec[w * L + lane] = (uint8_t)y;
-          const uint32_t v = wt[(j * kWarps + w) * L + y];
+          const uint32_t v = (L <= 4u && s_dense[set][j * kWarps + w]) ? dense_region_entry(y, L)
+                                                                       : wt[(j * kWarps + w) * L + y];
           cnt += v & 0xFFFFu;
           y = v >> 16;
         }
@@ -2255,7 +2255,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         if (whole && lane < L) {
 #pragma unroll
           for (uint32_t w = 0; w < (uint32_t)kWarps; ++w) {
-            const uint32_t v = wt[(j * kWarps + w) * L + lane];  // region w from carry `lane`
+            const uint32_t v = (L <= 4u && s_dense[set][j * kWarps + w])  // region w from carry `lane`
+                                   ? dense_region_entry(lane, L)
+                                   : wt[(j * kWarps + w) * L + lane];
             const uint32_t wc = v & 0xFFFFu, co = v >> 16;
             if (2048u - lane - wc * L + co != 0u) {
               bad = true;
@@ -2446,7 +2448,8 @@ __global__ void __launch_bounds__(kThreads, 3)
         } else {
           const uint32_t cs = subrec_b[jr * L + cin];
           const uint32_t cw = wrec_b[(jr * kWarps + wr) * L + cs];
-          const uint32_t e = reinterpret_cast<const uint32_t*>(wtab_b)[(jr * kWarps + wr) * L + cw];
+          const uint32_t e = (L <= 4u && s_dense[set][lane]) ? dense_region_entry(cw, L)
+                                                               : reinterpret_cast<const uint32_t*>(wtab_b)[lane * L + cw];
           wc = e & 0xFFFFu;
           olen_r = 2048u - cw - wc * L + (e >> 16) + wc * R;
           x0 = cw;
@@ -2528,7 +2531,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         uint32_t cw = 0;
         if (lane < 8u) {
           cw = wrec[lane * L + cs];
-          const uint32_t e = wt[lane * L + cw];
+          const uint32_t e = (L <= 4u && s_dense[set][j * kWarps + lane]) ? dense_region_entry(cw, L) : wt[lane * L + cw];
           const uint32_t wc = e & 0xFFFFu, co = e >> 16;
           wolen = wbytes - (cw < wbytes ? cw : wbytes) - wc * L + co + wc * R;
           ewc = wc;
@@ -2606,7 +2609,8 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
       } else {
         const uint32_t mycw = __shfl_sync(0xffffffffu, covs_l, warp);
-        x_in = (srec_b)[((size_t)j * kThreads + tid) * L + mycw];
+        x_in = (L <= 4u && s_dense[set][j * kWarps + warp]) ? dense_seg_carry(mycw, lane * 64u, L)
+                                                            : (srec_b)[((size_t)j * kThreads + tid) * L + mycw];
         if (x_in < 64u) {
           const Walk w = seg_walk(mask, x_in, L, p.inv_l, p.stride_mask);
           kept = w.kept;
