@@ -1686,6 +1686,8 @@ __device__ __forceinline__ void ks_compose_n(uint32_t& t0, uint32_t& t1, uint32_
 
 // Kogge-Stone scan of the warp's 32 segment functions (L = LL <= 4): srec row of this
 // segment (carry into it for each warp carry-in) and, from lane 31, the warp function.
+// *dense (written by lane 0) tells whether the region is all candidates; then no table is
+// written and every reader uses the closed forms.
 template <int LL>
 __device__ __forceinline__ void ks_warp_tables(uint64_t mask, uint32_t inv_l, uint64_t stride, uint8_t* srec_row,
                                                uint32_t* wtab_row, uint8_t* dense) {
