@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import hashlib
 import json
 import os
 import statistics
@@ -58,7 +59,12 @@ def parse_args(argv=None):
                     help="single: the single-pair workload (default line); chain: 4 GiB text x 128 pairs "
                          "through apply_batch; stream: 16 GiB text x 8 pairs through gpu_replace_streaming")
     ap.add_argument("--gib", type=float, default=0.0, help="input GiB of the chain/stream workloads (0 = 4 / 16)")
-    ap.add_argument("--jobs", type=int, default=160, help="jobs in the batched/served sample")
+    ap.add_argument("--jobs", type=int, default=500, help="jobs in the batched/served sample")
+    ap.add_argument("--rates", default="0.25,0.5,0.75,0.9",
+                    help="Poisson arrival rates of the served sample, as fractions of the closed-loop rate")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other workloads' figures (16 MiB one-shot, 4 GiB 128-pair chain, "
+                         "16 GiB streaming, pageable-input unified)")
     return ap.parse_args(argv)
 
 
@@ -333,6 +339,17 @@ def run_ours(args, dist: Dist):
     if not args.no_batched:
         batched = run_batched(args, lib)
 
+    extra = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_extra:
+        del outs, d_run, d_rand
+        torch.cuda.empty_cache()
+        outs = d_run = d_rand = None
+        extra = {"c1_one_shot": c1_figures(lib, dev),
+                 "e2e_pageable": pageable_e2e(lib, n_run, rand_np),
+                 "chain_128_pairs": chain_figures(lib, 4 * GiB if args.scale >= 1.0 else int(256 * MiB * args.scale) + MiB,
+                                                  2, 1),
+                 "stream_8_pairs": stream_figures(lib, 16 * GiB if args.scale >= 1.0 else int(GiB * args.scale) + MiB, 1)}
+
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         cb, ct, desc = cpu_sample(rand_np, min(args.scale, 1.0))
@@ -365,6 +382,8 @@ def run_ours(args, dist: Dist):
             line["e2e"] = e2e
         if batched:
             line["batched"] = batched
+        if extra:
+            line["extra"] = extra
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -374,11 +393,13 @@ def run_ours(args, dist: Dist):
 
 
 def run_batched(args, lib):
-    """Batched/served jobs: a sample of the 10,000-job workload (same generator: sizes
-    log-uniform 4 KiB-64 MiB, per-job alphabets of 4-64 symbols, 1-16 pairs with pattern 1-32 B
-    and replacement 0-64 B), through the request loop (cuda_replace_server_*) against the same
-    jobs issued one by one as plain unified() calls (one call per pair). Closed loop (all jobs
-    submitted at once) for jobs/s, then Poisson arrivals at half that rate for latency."""
+    """Batched/served jobs: the first --jobs jobs of the 10,000-job workload (same generator:
+    sizes log-uniform 4 KiB-64 MiB, per-job alphabets of 4-64 symbols, 1-16 pairs with pattern
+    1-32 B and replacement 0-64 B) through the request loop (cuda_replace_server_*), against the
+    SAME jobs issued one by one as plain unified() calls (one call per pair). Each arm runs one
+    untimed pass over all jobs first. Closed loop (all jobs submitted at once) gives jobs/s;
+    Poisson arrivals at each rate of --rates (fractions of the closed-loop rate) give p50/p99
+    latency from submit to result. Every result is compared with the unified() arm's."""
     import random
 
     from cuda_replace_b200 import workloads as WL
@@ -387,6 +408,7 @@ def run_batched(args, lib):
     jobs = [WL.c5_job(i) for i in range(args.jobs)]
     n_bytes = sum(len(j.data) for j in jobs)
     out = {"jobs": len(jobs), "input_bytes": n_bytes}
+    fracs = [float(x) for x in args.rates.split(",") if x]
     with Server(lib) as srv:
         # warm-up: one untimed pass over all jobs (tuning, graphs, staging, and the host pages
         # the results land in: first-touch page faults would otherwise dominate the figure)
@@ -403,44 +425,58 @@ def run_batched(args, lib):
                     "closed_loop_p50_ms": round(st["p50_us"] / 1e3, 3), "closed_loop_p99_ms": round(st["p99_us"] / 1e3, 3),
                     "batches": st["batches"], "jobs_via_session": st["jobs_via_session"],
                     "tile_bytes": st["tile_bytes"], "grid_ctas": st["grid_ctas"]})
-        # open loop: Poisson arrivals at half the closed-loop rate
-        lam = 0.5 * rate
-        rng = random.Random(5)
-        srv.reset_stats()
-        t_start = time.perf_counter()
-        t_next = t_start
-        tickets = []
+        # open loop: Poisson arrivals at fractions of the closed-loop rate
+        sweep = []
+        for frac in fracs:
+            lam = frac * rate
+            rng = random.Random(5)
+            srv.reset_stats()
+            t_start = time.perf_counter()
+            t_next = t_start
+            tickets = []
+            for j in jobs:
+                t_next += rng.expovariate(lam)
+                d = t_next - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets.append(srv.submit(j.data, j.pairs))
+            for t in tickets:
+                srv.wait(t)
+            span = time.perf_counter() - t_start
+            st = srv.stats()
+            sweep.append({"rate_frac": frac, "arrival_jobs_per_s": round(lam, 2),
+                          "served_jobs_per_s": round(len(jobs) / span, 2),
+                          "p50_ms": round(st["p50_us"] / 1e3, 3), "p99_ms": round(st["p99_us"] / 1e3, 3)})
+        out["poisson"] = sweep
+    # the same jobs as per-job plain unified() calls, after the same kind of warm pass
+    def unified_all():
+        res = []
         for j in jobs:
-            t_next += rng.expovariate(lam)
-            d = t_next - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            tickets.append(srv.submit(j.data, j.pairs))
-        for t in tickets:
-            srv.wait(t)
-        st = srv.stats()
-        out.update({"poisson_rate_jobs_per_s": round(lam, 2), "p50_ms": round(st["p50_us"] / 1e3, 3),
-                    "p99_ms": round(st["p99_us"] / 1e3, 3)})
-    # per-job plain unified() on a prefix of the same jobs (after the same kind of warm pass)
-    m = min(len(jobs), max(8, len(jobs) // 6))
-    for j in jobs[:m]:
-        d = j.data
-        for p, r in j.pairs:
-            d = lib.unified(d, p, r)
-    del d
+            d = j.data
+            for p, r in j.pairs:
+                d = lib.unified(d, p, r)
+            res.append(d)
+        return res
+    base = unified_all()
+    del base
     t0 = time.perf_counter()
-    base = []
-    for j in jobs[:m]:
-        d = j.data
-        for p, r in j.pairs:
-            d = lib.unified(d, p, r)
-        base.append(d)
+    base = unified_all()
     ub = time.perf_counter() - t0
-    if any(outs[i] != base[i] for i in range(m)):
-        raise SystemExit("batched self-check failed: results differ from per-job unified()")
-    out["unified_jobs_per_s"] = round(m / ub, 2)
-    out["unified_sample_jobs"] = m
-    out["speedup_vs_unified"] = round(rate / (m / ub), 2)
+    bad = [j.job_id for j, a, b_ in zip(jobs, outs, base) if a != b_]
+    if bad:
+        raise SystemExit(f"batched self-check failed: jobs {bad[:8]} differ from per-job unified()")
+    out["unified_jobs_per_s"] = round(len(jobs) / ub, 2)
+    out["unified_same_jobs"] = True
+    out["speedup_vs_unified"] = round(rate / (len(jobs) / ub), 2)
+    golden = load_fullsize().get("c5", {}).get("jobs", [])
+    checked = 0
+    for j, o in zip(jobs, outs):
+        if j.job_id < len(golden):
+            g = golden[j.job_id]
+            if len(o) != g["out_len"] or hashlib.sha256(o).hexdigest() != g["out_sha256"]:
+                raise SystemExit(f"batched digest check failed for job {j.job_id}")
+            checked += 1
+    out["digests_checked"] = checked
     return out
 
 
@@ -484,84 +520,174 @@ def run_e2e(args, lib, n_run, rand_np, dist: Dist, dev, sel):
             "steps": steps, "api": "cuda_replace_unified (page-locked host input)"}
 
 
-def tiled_text(total: int, seed: int):
-    """total bytes of the Zipf text generator: a 256 MiB generated block repeated (generating
-    16 GiB directly would take minutes)."""
+def load_fullsize() -> dict:
+    """Digests of the chained bytes.replace output at full size (tests/golden/fullsize.json,
+    made by tests/golden/make_fullsize.py)."""
+    p = REPO / "tests" / "golden" / "fullsize.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def chain_figures(lib, total: int, steps: int, warmup: int) -> dict:
+    """The 128-pair chain on tiled Zipf text (4 GiB at full size) with Session.apply_batch:
+    every pair one launch, lengths chained on the device, one read-back per chain. Device
+    figure: sum over passes of (input + output) bytes / the apply_batch call (input resident in
+    HBM). End to end: host bytes in (reset) -> apply_batch -> host bytes out (result). The
+    result's SHA-256 is checked against the full-size digest."""
     from cuda_replace_b200 import workloads as WL
-    base = WL.text_corpus(min(total, 256 * MiB), seed=seed)
-    reps = total // len(base) + 1
-    return (base * reps)[:total]
+    from cuda_replace_b200.cuda_replace_wrapper import Session
+    txt, pairs = WL.c3_input(total, seed=3)
+    with Session(lib, txt) as s:
+        lens = [len(txt)]
+        for p, r in pairs:  # pass lengths, for the algorithmic bytes (also a warm pass)
+            lens.append(s.apply(p, r))
+        algo = sum(lens[k] + lens[k + 1] for k in range(len(pairs)))
+        dev_t, e2e_t = [], []
+        out = None
+        for it in range(max(warmup, 1) + max(steps, 1)):
+            t0 = time.perf_counter()
+            s.reset(txt)
+            t1 = time.perf_counter()
+            n = s.apply_batch(pairs)
+            t2 = time.perf_counter()
+            out = s.result()
+            t3 = time.perf_counter()
+            if n != lens[-1] or len(out) != n:
+                raise SystemExit(f"chain self-check failed: {n} != {lens[-1]}")
+            if it >= max(warmup, 1):
+                dev_t.append(t2 - t1)
+                e2e_t.append(t3 - t0)
+        _, launches = s.stats()
+    g = load_fullsize().get("c3")
+    digest = "not checked (size differs from the digest's)"
+    if g and g["in_len"] == len(txt):
+        if len(out) != g["out_len"] or hashlib.sha256(out).hexdigest() != g["out_sha256"]:
+            raise SystemExit("chain digest check failed: output differs from the chained bytes.replace")
+        digest = "sha256 equal to the chained bytes.replace"
+    t, te = statistics.median(dev_t), statistics.median(e2e_t)
+    return {"workload": f"{total / GiB:g} GiB tiled Zipf text x 128 entity pairs, Session.apply_batch",
+            "gbs_sum_in_out": round(algo / t / 1e9, 2), "ms_per_chain": round(t * 1e3, 2),
+            "end_to_end_gbs": round((lens[0] + lens[-1]) / te / 1e9, 3), "end_to_end_ms": round(te * 1e3, 1),
+            "launches_per_chain": len(pairs), "final_len": lens[-1], "steps": len(dev_t), "check": digest,
+            "timer": "host clock around the synchronous call"}
+
+
+def stream_figures(lib, total: int, steps: int) -> dict:
+    """Streaming: tiled Zipf text (16 GiB at full size) with a pattern planted across every
+    256 MiB chunk boundary, 8 pairs, through gpu_replace_streaming (chunk-major: one
+    host-link crossing each way). The result's SHA-256 is checked against the full-size
+    digest."""
+    from cuda_replace_b200 import workloads as WL
+    from cuda_replace_b200.cuda_replace_wrapper import gpu_replace_streaming
+    chunk = 256 * MiB
+    buf, pairs, planted = WL.c4_input(total, chunk=chunk, seed=4)
+    times, out = [], None
+    for it in range(1 + max(steps, 1)):
+        out = None
+        t0 = time.perf_counter()
+        out = gpu_replace_streaming(lib, buf, pairs, chunk_bytes=chunk)
+        dt = time.perf_counter() - t0
+        if it >= 1:
+            times.append(dt)
+    g = load_fullsize().get("c4")
+    digest = "not checked (size differs from the digest's)"
+    if g and g["in_len"] == len(buf):
+        if len(out) != g["out_len"] or hashlib.sha256(out).hexdigest() != g["out_sha256"]:
+            raise SystemExit("stream digest check failed: output differs from the chained bytes.replace")
+        digest = "sha256 equal to the chained bytes.replace"
+    t = statistics.median(times)
+    return {"workload": f"{total / GiB:g} GiB tiled Zipf text x 8 pairs, chunk 256 MiB, "
+                        f"{planted} patterns planted across chunk boundaries",
+            "input_gbs": round(total / t / 1e9, 3), "ms": round(t * 1e3, 1),
+            "h2d_bytes": total, "d2h_bytes": len(out), "host_link_gbs": round((total + len(out)) / t / 1e9, 3),
+            "api": "gpu_replace_streaming (Python bytes in, Python bytes out)", "steps": len(times),
+            "check": digest}
+
+
+def c1_figures(lib, dev) -> dict:
+    """16 MiB one-shot ACGT -> N: launch-bound. Device: one launch on a resident input, CUDA
+    events over 50 launches. Host: unified() from Python bytes to Python bytes."""
+    import torch
+
+    from cuda_replace_b200 import workloads as WL
+    from cuda_replace_b200.cuda_replace_wrapper import Session
+    src, pat, rep = WL.c1_acgt(16 * MiB, seed=1)
+    want = src.replace(pat, rep)
+    n = len(src)
+    d_in = torch.empty(n + 64, dtype=torch.uint8, device=dev)
+    d_in[:n].copy_(torch.frombuffer(bytearray(src), dtype=torch.uint8))
+    d_out = torch.empty(n + 64, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    with Session(lib, b"") as s:
+        for _ in range(5):
+            s.apply_device_async(d_in.data_ptr(), n, pat, rep, d_out.data_ptr(), n, stream.cuda_stream)
+        out_len, _ = s.device_result()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 50
+        ev0.record(stream)
+        for _ in range(reps):
+            s.apply_device_async(d_in.data_ptr(), n, pat, rep, d_out.data_ptr(), n, stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        dev_us = ev0.elapsed_time(ev1) * 1e3 / reps
+    if out_len != len(want) or bytes(d_out[:out_len].cpu().numpy()) != want:
+        raise SystemExit("C1 self-check failed")
+    for _ in range(3):
+        lib.unified(src, pat, rep)
+    t0 = time.perf_counter()
+    calls = 20
+    for _ in range(calls):
+        got = lib.unified(src, pat, rep)
+    host_us = (time.perf_counter() - t0) * 1e6 / calls
+    if got != want:
+        raise SystemExit("C1 unified self-check failed")
+    return {"workload": "16 MiB i.i.d. ACGT, ACGT -> N (one launch)", "device_us": round(dev_us, 1),
+            "device_gbs": round((n + out_len) / dev_us / 1e3, 1), "unified_us": round(host_us, 1),
+            "unified_gbs": round((n + out_len) / host_us / 1e3, 2)}
+
+
+def pageable_e2e(lib, n_run: int, rand_np) -> dict:
+    """The single-pair step through the reference wrapper's call shape: CudaReplaceLib.unified
+    on Python bytes (pageable host memory), result returned as Python bytes."""
+    srcs = [b"a" * n_run, b"a" * n_run, rand_np.tobytes()]
+    total = 0
+    for (_, p, r), src in zip(CASES, srcs):  # warm pass
+        total += len(src) + len(lib.unified(src, p, r))
+    steps = 2
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for (_, p, r), src in zip(CASES, srcs):
+            out = lib.unified(src, p, r)
+            del out
+    secs = time.perf_counter() - t0
+    return {"value": round(total * steps / secs / 1e9, 3), "unit": "GB/s", "steps": steps,
+            "h2d_bytes_per_step": sum(len(x) for x in srcs), "d2h_bytes_per_step": total - sum(len(x) for x in srcs),
+            "api": "CudaReplaceLib.unified(bytes) -> bytes (pageable host memory)"}
 
 
 def run_chain(args):
-    """4 GiB text, 128 entity pairs applied in order with Session.apply_batch (lengths chained
-    on the device). Metric: GB/s of sum over passes of (input + output) bytes, input resident."""
-    from cuda_replace_b200 import workloads as WL
-    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib, Session
+    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib
     lib = CudaReplaceLib()
     total = int((args.gib or 4.0) * GiB)
-    txt = tiled_text(total, seed=3)
-    pairs = WL.c3_pairs(seed=3)
-    with Session(lib, txt) as s:
-        lens = [len(txt)]
-        for p, r in pairs:  # pass lengths, for the algorithmic bytes
-            lens.append(s.apply(p, r))
-        algo = sum(lens[k] + lens[k + 1] for k in range(len(pairs)))
-        times = []
-        for it in range(max(args.warmup, 1) + max(args.steps, 1)):
-            s.reset(txt)
-            t0 = time.perf_counter()
-            n = s.apply_batch(pairs)
-            dt = time.perf_counter() - t0
-            if n != lens[-1]:
-                raise SystemExit(f"chain self-check failed: {n} != {lens[-1]}")
-            if it >= max(args.warmup, 1):
-                times.append(dt)
-        _, launches = s.stats()
-    t = statistics.median(times)
-    line = {"metric": "GB/s (sum over passes of in+out), 128-pair chain", "value": round(algo / t / 1e9, 2),
-            "unit": "GB/s", "n_gpus": 1, "steps": len(times), "warmup": max(args.warmup, 1),
-            "ms_per_step": round(t * 1e3, 3), "higher_is_better": True, "dtype": "u8",
-            "data": "synthetic (Zipf text, 256 MiB generated block repeated)",
-            "config": {"workload": f"{total / GiB:g} GiB text x 128 entity pairs, Session.apply_batch",
-                       "end_to_end_gbs": round((lens[0] + lens[-1]) / t / 1e9, 3), "final_len": lens[-1]},
-            "gpu_launches_per_step": len(pairs)}
+    f = chain_figures(lib, total, args.steps, args.warmup)
+    line = {"metric": "GB/s (sum over passes of in+out), 128-pair chain", "value": f["gbs_sum_in_out"],
+            "unit": "GB/s", "n_gpus": 1, "steps": f["steps"], "warmup": max(args.warmup, 1),
+            "ms_per_step": f["ms_per_chain"], "higher_is_better": True, "dtype": "u8",
+            "data": "synthetic (Zipf text, 256 MiB generated block repeated)", "config": f,
+            "gpu_launches_per_step": f["launches_per_chain"]}
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_stream(args):
-    """16 GiB text, 8 pairs (L 2-16, R 0-32), 256 MiB chunks, matches planted across every chunk
-    boundary, through gpu_replace_streaming (chunk-major: one host-link crossing each way)."""
-    from cuda_replace_b200 import workloads as WL
-    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib, gpu_replace_streaming
+    from cuda_replace_b200.cuda_replace_wrapper import CudaReplaceLib
     lib = CudaReplaceLib()
     total = int((args.gib or 16.0) * GiB)
-    chunk = 256 * MiB
-    txt = tiled_text(total, seed=4)
-    pairs = WL.c4_pairs(seed=4)
-    planted = 0
-    for pat, _ in pairs[:4]:
-        txt, c = WL.plant_across_boundaries(txt, pat, chunk, seed=len(pat))
-        planted += c
-    times = []
-    out_len = 0
-    for it in range(1 + max(args.steps, 1)):
-        t0 = time.perf_counter()
-        out = gpu_replace_streaming(lib, txt, pairs, chunk_bytes=chunk)
-        dt = time.perf_counter() - t0
-        out_len = len(out)
-        del out
-        if it >= 1:
-            times.append(dt)
-    t = statistics.median(times)
+    f = stream_figures(lib, total, args.steps)
     line = {"metric": "GB/s of input, 8-pair streaming (host bytes in, host bytes out)",
-            "value": round(total / t / 1e9, 3), "unit": "GB/s", "n_gpus": 1, "steps": len(times), "warmup": 1,
-            "ms_per_step": round(t * 1e3, 1), "higher_is_better": True, "dtype": "u8",
+            "value": f["input_gbs"], "unit": "GB/s", "n_gpus": 1, "steps": f["steps"], "warmup": 1,
+            "ms_per_step": f["ms"], "higher_is_better": True, "dtype": "u8",
             "data": "synthetic (Zipf text, 256 MiB generated block repeated, matches planted at every chunk boundary)",
-            "config": {"workload": f"{total / GiB:g} GiB text x 8 pairs, chunk 256 MiB", "planted": planted,
-                       "h2d_bytes": total, "d2h_bytes": out_len,
-                       "host_link_gbs": round((total + out_len) / t / 1e9, 3)}}
+            "config": f}
     print(json.dumps(line), flush=True)
     return 0
 

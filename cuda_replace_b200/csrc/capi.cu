@@ -138,6 +138,9 @@ struct Session {
   size_t lens_cap = 0;
   cudaStream_t async_stream = nullptr;  // stream of the last cuda_replace_apply_device_async
   uint32_t async_epoch = 0;
+  bool async_copy = false;          // the last async call copied its input (n < pattern length)
+  unsigned long long async_n = 0;   // ... and this many bytes
+  cudaEvent_t ev_order = nullptr;   // orders the session stream and a caller stream
 
   // the most recent apply, for query_prefix: 0 none, 1 no match possible, 2 kernel, 3 empty pattern
   int q_kind = 0;
@@ -277,6 +280,7 @@ void session_free(Session* s) {
     cudaStreamSynchronize(s->down);
     cudaStreamDestroy(s->down);
   }
+  if (s->ev_order) cudaEventDestroy(s->ev_order);
   if (s->carry2) cudaFree(s->carry2);
   if (s->olen_dev) cudaFree(s->olen_dev);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -862,12 +866,28 @@ CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size
                                                int pat_len, const uint8_t* rep, int rep_len, uint8_t* d_out,
                                                size_t out_cap, void* stream) {
   SESSION_GUARD(h);
-  if (pat_len <= 0 || rep_len < 0 || (size_t)pat_len > n) return -1;
+  if (pat_len <= 0 || rep_len < 0) return -1;
   if (pat_len > crb::kInlineMax || rep_len > crb::kInlineMax) return -4;
   if ((n && !d_in) || !d_out || !pat || (rep_len && !rep)) return -1;
   if (((uintptr_t)d_in & 15u) || ((uintptr_t)d_out & 15u)) return (int)cudaErrorInvalidValue;
   const uint32_t L = (uint32_t)pat_len, R = (uint32_t)rep_len;
   if (out_cap < output_bound(n, L, R)) return (int)cudaErrorInvalidValue;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  cudaError_t e = cudaSuccess;
+  if (!s->ev_order) {
+    e = cudaEventCreateWithFlags(&s->ev_order, cudaEventDisableTiming);
+    if (e != cudaSuccess) return (int)e;
+  }
+  if ((size_t)L > n) {  // no occurrence possible: the output is the input, as bytes.replace gives
+    if (n) e = cudaMemcpyAsync(d_out, d_in, n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return (int)e;
+    s->async_stream = st;
+    s->async_epoch = 1;
+    s->async_copy = true;
+    s->async_n = n;
+    s->q_kind = 0;
+    return 0;
+  }
   ReplaceParams p;
   memset(&p, 0, sizeof(p));
   crb::prepare_pattern_fields(p, pat, L);
@@ -877,7 +897,7 @@ CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size
   const size_t tiles = (n + tile_bytes - 1) / tile_bytes;
   if (tiles > 0xFFFFFFF0ull) return (int)cudaErrorInvalidValue;
   p.num_tiles = (uint32_t)tiles;
-  cudaError_t e = ensure_scratch(s, tiles, p.agg_entries);
+  e = ensure_scratch(s, tiles, p.agg_entries);
   if (e != cudaSuccess) return (int)e;
   p.tile_last = s->tile_last;
   p.rec = s->rec;
@@ -892,12 +912,25 @@ CR_EXPORT int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size
   p.agg = s->agg;
   p.res = s->res;
   p.epoch = next_epoch(s);
-  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  if (st != s->stream) {
+    // ensure_scratch and next_epoch clear look-back scratch on the session stream: the kernel
+    // on the caller's stream must not start before those clears have landed.
+    e = cudaEventRecord(s->ev_order, s->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, s->ev_order, 0);
+    if (e != cudaSuccess) return (int)e;
+  }
   e = p.nsub ? crb::launch_replace_super(p, st, nullptr) : crb::launch_replace(p, st, nullptr);
   if (e != cudaSuccess) return (int)e;
   ++s->launches;
+  if (st != s->stream) {
+    // later work of this handle on its own stream (clears, other applies) waits for the kernel
+    e = cudaEventRecord(s->ev_order, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->stream, s->ev_order, 0);
+    if (e != cudaSuccess) return (int)e;
+  }
   s->async_stream = st;
   s->async_epoch = p.epoch;
+  s->async_copy = false;
   s->q_kind = 0;
   return 0;
 }
@@ -907,7 +940,13 @@ CR_EXPORT int cuda_replace_device_result(void* h, size_t* out_len, unsigned long
   if (!s->async_epoch) return -1;
   cudaStream_t st = s->async_stream ? s->async_stream : s->stream;
   cudaError_t e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) e = cudaMemcpy(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return (int)e;
+  if (s->async_copy) {
+    if (out_len) *out_len = (size_t)s->async_n;
+    if (kept) *kept = 0;
+    return 0;
+  }
+  e = cudaMemcpy(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return (int)e;
   const ApplyResult r = *s->res_host;
   if (r.error_epoch == s->async_epoch || r.overflow_epoch == s->async_epoch) return kErrUnknown;
@@ -931,21 +970,21 @@ CR_EXPORT void cuda_replace_close(void* h) {
 // chunk's upload is queued at once; each chunk is replaced as soon as it is on the device (its
 // last L - 1 bytes held back for the next chunk, the coverage carried across on the device)
 // into the session's output buffer, and its output is downloaded into the result while the
-// next chunks upload. Returns 1 when the call does not qualify (the caller takes the
-// single-launch path), else 0 or an error.
+// next chunks upload. Returns kFallback when the call does not qualify (the caller takes the
+// single-launch path), else 0 or an error code (a cudaError_t, or 999).
 int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat, uint32_t L, const uint8_t* rep,
                     uint32_t R, uint8_t** out_host, size_t* out_len) {
   if (n < kUnifiedChunkedMin || L == 0 || L > (uint32_t)crb::kInlineMax || R > (uint32_t)crb::kInlineMax ||
       !host_is_pinned(src))
-    return 1;
+    return kFallback;
   ReplaceParams proto;
   memset(&proto, 0, sizeof(proto));
   crb::prepare_pattern_fields(proto, pat, L);
   proto.R = R;
   proto.nsub = crb::super_nsub(proto.mode, L);
-  if (!proto.nsub) return 1;
+  if (!proto.nsub) return kFallback;
   const size_t bound = output_bound(n, L, R);
-  if (bound > 4 * n + ((size_t)64 << 20)) return 1;  // a large expansion: the single-launch path sizes it
+  if (bound > 4 * n + ((size_t)64 << 20)) return kFallback;  // a large expansion: the single-launch path sizes it
   memcpy(proto.pat, pat, L);
   if (R) memcpy(proto.rep, rep, R);
   const size_t P = L - 1;  // bytes held back at the end of every chunk but the last
@@ -954,7 +993,7 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   // replace then starts P bytes earlier, at k * chunk, a 16-byte boundary as the loads need.
   size_t nchunks = (n + chunk - 1) / chunk;
   while (nchunks > 1 && (nchunks - 1) * chunk + P >= n) --nchunks;
-  if (nchunks > (size_t)kUnifiedChunks) return 1;
+  if (nchunks > (size_t)kUnifiedChunks) return kFallback;
   auto bnd = [&](size_t k) -> size_t { return k == 0 ? 0 : (k >= nchunks ? n : k * chunk + P); };
   const size_t tile_bytes = (size_t)crb::kTile * proto.nsub;
 
@@ -975,7 +1014,7 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   uint8_t* host = static_cast<uint8_t*>(pinned_pool().get(bound ? bound : 1, &e));
   if (!host) {
     cudaGetLastError();  // a page-locked block of the worst case was refused: the single-launch
-    return 1;            // path allocates the result at its exact size
+    return kFallback;            // path allocates the result at its exact size
   }
   for (size_t k = 0; k < nchunks && e == cudaSuccess; ++k) {
     const size_t a = bnd(k), m = bnd(k + 1) - a;
@@ -1065,7 +1104,7 @@ CR_EXPORT int cuda_replace_unified(const uint8_t* src, size_t src_len, const uin
   }
   if (pat_len > 0 && rep_len >= 0 && pat && (rep || rep_len == 0)) {
     rc = unified_chunked(s, src, src_len, pat, (uint32_t)pat_len, rep, (uint32_t)rep_len, out_host, out_len);
-    if (rc != 1) {
+    if (rc != kFallback) {
       if (rc == 0) {
         cache_give(s);
       } else {

@@ -156,6 +156,49 @@ def c4_pairs(seed: int = 4) -> List[Pair]:
     return pairs
 
 
+def tiled_text(total: int, seed: int, block: int = 256 * MiB) -> bytes:
+    """total bytes of the Zipf text: a generated block of `block` bytes (256 MiB, twice the
+    L2 cache) repeated and cut to length. This is the full-size input of the 128-pair chain
+    (4 GiB) and of the streaming workload (16 GiB): generating gigabytes of Zipf text directly
+    takes minutes."""
+    base = text_corpus(min(total, block), seed=seed)
+    if total <= len(base):
+        return base[:total]
+    k, rem = divmod(total, len(base))
+    return b"".join([base] * k + [base[:rem]])
+
+
+def c3_input(total: int = 4 * GiB, seed: int = 3) -> Tuple[bytes, List[Pair]]:
+    """The 128-pair chain workload: tiled Zipf text with entity tokens and the 128 pairs."""
+    return tiled_text(total, seed), c3_pairs(seed)
+
+
+def c4_input(total: int = 16 * GiB, chunk: int = 256 * MiB, seed: int = 4):
+    """The streaming workload: tiled Zipf text, the 8 mixed pairs, and at every multiple of
+    `chunk` the pattern of pair (j mod 8) written across boundary j (1 to L-1 of its bytes
+    before it), so every pair meets a match straddling a chunk boundary. Returns (bytearray,
+    pairs, planted); the buffer is planted in place (no copy of the whole input)."""
+    pairs = c4_pairs(seed)
+    base = text_corpus(min(total, 256 * MiB), seed=seed)
+    buf = bytearray(total)
+    view = memoryview(base)
+    for o in range(0, total, len(base)):
+        m = min(len(base), total - o)
+        buf[o:o + m] = view[:m]
+    rng = np.random.default_rng(seed + 7)
+    planted = 0
+    for j, b in enumerate(range(chunk, len(buf), chunk)):
+        pat = pairs[j % len(pairs)][0]
+        L = len(pat)
+        off = int(rng.integers(1, L))
+        s = b - off
+        if s < 0 or s + L > len(buf):
+            continue
+        buf[s:s + L] = pat
+        planted += 1
+    return buf, pairs, planted
+
+
 def plant_across_boundaries(data: bytes, pat: bytes, chunk: int, seed: int = 4) -> Tuple[bytes, int]:
     """Overwrite bytes so that pat occurs straddling every multiple of chunk. Returns (data, count)."""
     rng = np.random.default_rng(seed)

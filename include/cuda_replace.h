@@ -135,8 +135,11 @@ int cuda_replace_stats(void* h, unsigned long long* kept_last_apply,
  * NULL = the session's own stream) without waiting for it. d_in and d_out must be 16-byte
  * aligned device pointers, d_in readable up to n rounded up to 16, and out_cap at least
  * the worst-case output n + (n / pat_len) * max(0, rep_len - pat_len). pat_len must be in
- * [1, 256] and rep_len in [0, 256]. Calls on one handle must use one stream (they share the
- * handle's look-back scratch). The session buffer is not touched. */
+ * [1, 256] and rep_len in [0, 256]. When n < pat_len no occurrence is possible and d_in is
+ * copied to d_out unchanged (as bytes.replace returns its input). Calls on one handle must use
+ * one stream (they share the handle's look-back scratch); the handle's own stream is ordered
+ * around the launch by events, so its scratch clears never overlap the kernel. The session
+ * buffer is not touched. */
 int cuda_replace_apply_device_async(void* h, const uint8_t* d_in, size_t n,
                                     const uint8_t* pat, int pat_len,
                                     const uint8_t* rep, int rep_len,

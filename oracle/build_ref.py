@@ -2,7 +2,12 @@
 
 Recipe: copy the reference source ``cuda_replace.cu`` (RAZZULLIX/cuda_replace) into
 ``oracle/_ref/`` (git-ignored, never committed), apply a purely mechanical patch, and
-compile it with nvcc into ``oracle/_ref/libcuda_replace_ref.so``.
+compile it with nvcc into ``oracle/_ref/libcuda_replace_ref.so``. The reference's ctypes
+wrapper ``cuda_replace_wrapper.py`` is copied beside it unchanged, so the GPU parity tests
+drive both libraries through the reference's own binding.
+
+The reference checkout is read from ``--ref-dir DIR``, else from the environment variable
+``CUDA_REPLACE_REF_DIR``, else from ``/root/reference`` (where this build machine mounts it).
 
 Why a patch is needed: the reference's error macros jump with ``goto cuda_fail`` over
 initialised local declarations (e.g. cuda_replace.cu:370-371, 1013, 1051), which MSVC
@@ -18,6 +23,7 @@ inputs inside its envelope (n, kept and output below 2**31).
 """
 from __future__ import annotations
 
+import os
 import re
 import shutil
 import subprocess
@@ -25,10 +31,12 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference/cuda_replace.cu")
+REF_DIR = Path(os.environ.get("CUDA_REPLACE_REF_DIR", "/root/reference"))
+REF_SRC = REF_DIR / "cuda_replace.cu"
 OUT_DIR = HERE / "_ref"
 PATCHED = OUT_DIR / "cuda_replace_ref.cu"
 LIB = OUT_DIR / "libcuda_replace_ref.so"
+WRAPPER = OUT_DIR / "cuda_replace_wrapper.py"
 NVCC_FLAGS = ["-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
               "-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -106,13 +114,24 @@ def _patch_decl(lines: list[str], idx: int) -> None:
         lines[k] = ""
 
 
-def build_reference(force: bool = False, verbose: bool = True) -> Path:
+def _copy_wrapper(ref_dir: Path) -> None:
+    src = ref_dir / "cuda_replace_wrapper.py"
+    if src.exists() and (not WRAPPER.exists() or WRAPPER.read_bytes() != src.read_bytes()):
+        shutil.copyfile(src, WRAPPER)
+
+
+def build_reference(force: bool = False, verbose: bool = True, ref_dir: Path | None = None) -> Path:
+    ref_dir = Path(ref_dir) if ref_dir is not None else REF_DIR
+    ref_src = ref_dir / "cuda_replace.cu"
     if LIB.exists() and not force:
+        if ref_dir.exists():
+            _copy_wrapper(ref_dir)
         return LIB
-    if not REF_SRC.exists():
-        raise FileNotFoundError(f"reference source not found: {REF_SRC}")
+    if not ref_src.exists():
+        raise FileNotFoundError(f"reference source not found: {ref_src}")
     OUT_DIR.mkdir(parents=True, exist_ok=True)
-    lines = REF_SRC.read_text().split("\n")
+    _copy_wrapper(ref_dir)
+    lines = ref_src.read_text().split("\n")
     for _ in range(6):
         PATCHED.write_text("\n".join(lines))
         err = _compile(PATCHED, LIB)
@@ -133,4 +152,9 @@ def build_reference(force: bool = False, verbose: bool = True) -> Path:
 
 
 if __name__ == "__main__":
-    build_reference(force="--force" in sys.argv)
+    import argparse
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--ref-dir", default=None, help="reference checkout (holds cuda_replace.cu)")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    build_reference(force=a.force, ref_dir=Path(a.ref_dir) if a.ref_dir else None)

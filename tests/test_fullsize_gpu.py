@@ -4,6 +4,7 @@ on the host are checked through size-independent properties on the device: exact
 length, periodicity of the replacement stream, and a SHA-256 against the C oracle where the
 oracle finishes in seconds. torch only provides device memory and the comparisons."""
 import hashlib
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -84,3 +85,64 @@ def test_session_chain_on_device_matches_oracle(cr_lib, torch_cuda):
         n = s.apply_batch(pairs)
         out = s.result()
     assert n == len(exp) and out == exp
+
+
+# ------------------------------------------------------------------ full stated sizes
+FULLSIZE = Path(__file__).parent / "golden" / "fullsize.json"
+
+
+def _fullsize(key):
+    import json
+    if not FULLSIZE.exists():
+        pytest.fail("tests/golden/fullsize.json is missing (python tests/golden/make_fullsize.py)")
+    doc = json.loads(FULLSIZE.read_text())
+    if key not in doc:
+        pytest.fail(f"tests/golden/fullsize.json has no '{key}' row")
+    return doc[key]
+
+
+def _sha_len(b):
+    return len(b), hashlib.sha256(b).hexdigest()
+
+
+def test_chain_4gib_128_pairs_digest(cr_lib):
+    """The 128-pair chain at its stated size: 4 GiB of tiled Zipf text, Session.apply_batch
+    (lengths chained on the device), output digest equal to the chained bytes.replace."""
+    g = _fullsize("c3")
+    txt, pairs = WL.c3_input(g["generator"]["total"], seed=g["generator"]["seed"])
+    assert len(txt) == g["in_len"]
+    with Wr.Session(cr_lib, txt) as s:
+        del txt
+        n = s.apply_batch(pairs)
+        out = s.result()
+    assert n == g["out_len"]
+    assert _sha_len(out) == (g["out_len"], g["out_sha256"])
+
+
+def test_stream_16gib_8_pairs_digest(cr_lib):
+    """Streaming at its stated size: 16 GiB of tiled Zipf text, a pattern planted across every
+    256 MiB chunk boundary, 8 mixed pairs, through gpu_replace_streaming (chunk-major native
+    path); output digest equal to the chained bytes.replace."""
+    g = _fullsize("c4")
+    gen = g["generator"]
+    buf, pairs, planted = WL.c4_input(gen["total"], chunk=gen["chunk"], seed=gen["seed"])
+    assert len(buf) == g["in_len"] and planted == g["planted"]
+    out = Wr.gpu_replace_streaming(cr_lib, buf, pairs, chunk_bytes=gen["chunk"])
+    del buf
+    assert _sha_len(out) == (g["out_len"], g["out_sha256"])
+
+
+def test_first_1000_jobs_served_digests(cr_lib):
+    """The first 1000 jobs of the batched-jobs generator at full size (4 KiB-64 MiB, 1-16 pairs
+    each) through the request loop; every job's output digest equal to its chained
+    bytes.replace."""
+    rows = _fullsize("c5")["jobs"]
+    assert len(rows) == 1000
+    with Wr.Server(cr_lib) as srv:
+        for lo in range(0, len(rows), 100):  # 100 jobs in flight at a time (bounded host memory)
+            jobs = [WL.c5_job(r["job_id"]) for r in rows[lo:lo + 100]]
+            tickets = [srv.submit(j.data, j.pairs) for j in jobs]
+            for j, t, r in zip(jobs, tickets, rows[lo:lo + 100]):
+                out = srv.wait(t)
+                assert (len(j.data), len(j.pairs)) == (r["in_len"], r["npairs"])
+                assert _sha_len(out) == (r["out_len"], r["out_sha256"]), f"job {r['job_id']}"

@@ -69,3 +69,34 @@ def test_noalloc_rejects_sizes_beyond_its_limits(cr_lib):
     assert rc == -6
     rc, _, _ = _noalloc(cr_lib, torch, d_in, 512, b"p" * 65, b"", 512)
     assert rc == -6
+
+
+def test_noalloc_at_its_size_limit_and_without_allocating(cr_lib):
+    """At the largest input the fixed scratch holds (every tile slot used) with a 64-byte
+    pattern that has a border (so each tile stores its full table of 64 carry entries): the
+    output equals bytes.replace and the existing entry point, on two calls in a row, and a
+    warm call leaves the device's free memory unchanged."""
+    import torch
+    n = 64 << 20
+    unit = b"ab" * 40 + b"x" + b"ab" * 31 + b"y"  # full and near matches of (ab)*32
+    data = (unit * (n // len(unit) + 1))[:n]
+    pat, rep = b"ab" * 32, b"Q"
+    d_in = _device(torch, data)
+    want = data.replace(pat, rep)
+    for _ in range(2):
+        rc, got, got_len = _noalloc(cr_lib, torch, d_in, n, pat, rep, n)
+        assert rc == 0 and got_len == len(want)
+        assert bytes(got[:got_len].cpu().numpy()) == want
+    ref, ref_len = _existing(cr_lib, torch, d_in, n, pat, rep, n)
+    assert ref_len == got_len and bool((ref[:ref_len] == got[:got_len]).all())
+    out = torch.empty(n + 64, dtype=torch.uint8, device="cuda")
+    fn = cr_lib.lib.cuda_replace_apply_device_noalloc
+    out_len = C.c_size_t(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    rc = fn(d_in.data_ptr(), n, pat, len(pat), rep, len(rep), out.data_ptr(), n, C.byref(out_len), stream)
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert rc == 0 and out_len.value == len(want)
+    assert free_after == free_before
