@@ -529,45 +529,68 @@ def load_fullsize() -> dict:
 
 def chain_figures(lib, total: int, steps: int, warmup: int) -> dict:
     """The 128-pair chain on tiled Zipf text (4 GiB at full size) with Session.apply_batch:
-    every pair one launch, lengths chained on the device, one read-back per chain. Device
-    figure: sum over passes of (input + output) bytes / the apply_batch call (input resident in
-    HBM). End to end: host bytes in (reset) -> apply_batch -> host bytes out (result). The
-    result's SHA-256 is checked against the full-size digest."""
+    lengths chained on the device, one read-back per chain. apply_batch runs each run of pairs
+    that the planner proved independent in one pass (multi-pattern stages); the same chain with
+    one pass per pair (CUDA_REPLACE_STAGES=0) is timed beside it. Device figure: the chain's
+    algorithmic bytes, sum over the 128 pairs of (input + output), / the apply_batch call
+    (input resident in HBM). End to end: host bytes in (reset) -> apply_batch -> host bytes out
+    (result). The result's SHA-256 is checked against the full-size digest."""
     from cuda_replace_b200 import workloads as WL
     from cuda_replace_b200.cuda_replace_wrapper import Session
     txt, pairs = WL.c3_input(total, seed=3)
+    res = {}
     with Session(lib, txt) as s:
         lens = [len(txt)]
         for p, r in pairs:  # pass lengths, for the algorithmic bytes (also a warm pass)
             lens.append(s.apply(p, r))
         algo = sum(lens[k] + lens[k + 1] for k in range(len(pairs)))
-        dev_t, e2e_t = [], []
         out = None
-        for it in range(max(warmup, 1) + max(steps, 1)):
-            t0 = time.perf_counter()
-            s.reset(txt)
-            t1 = time.perf_counter()
-            n = s.apply_batch(pairs)
-            t2 = time.perf_counter()
-            out = s.result()
-            t3 = time.perf_counter()
-            if n != lens[-1] or len(out) != n:
-                raise SystemExit(f"chain self-check failed: {n} != {lens[-1]}")
-            if it >= max(warmup, 1):
-                dev_t.append(t2 - t1)
-                e2e_t.append(t3 - t0)
-        _, launches = s.stats()
+        for arm, env in (("staged", None), ("per_pair", "0")):
+            if env is None:
+                os.environ.pop("CUDA_REPLACE_STAGES", None)
+            else:
+                os.environ["CUDA_REPLACE_STAGES"] = env
+            dev_t, e2e_t, launches = [], [], 0
+            nsteps = max(steps, 1) if arm == "staged" else 1
+            for it in range(max(warmup, 1) + nsteps):
+                t0 = time.perf_counter()
+                s.reset(txt)
+                t1 = time.perf_counter()
+                _, l0 = s.stats()
+                n = s.apply_batch(pairs)
+                t2 = time.perf_counter()
+                _, l1 = s.stats()
+                o = s.result()
+                t3 = time.perf_counter()
+                if n != lens[-1] or len(o) != n:
+                    raise SystemExit(f"chain self-check failed ({arm}): {n} != {lens[-1]}")
+                if it >= max(warmup, 1):
+                    dev_t.append(t2 - t1)
+                    e2e_t.append(t3 - t0)
+                    launches = l1 - l0
+                if arm == "staged":
+                    out = o
+                else:
+                    if o != out:
+                        raise SystemExit("chain self-check failed: staged and per-pair results differ")
+                del o
+            res[arm] = (statistics.median(dev_t), statistics.median(e2e_t), launches, len(dev_t))
+        os.environ.pop("CUDA_REPLACE_STAGES", None)
     g = load_fullsize().get("c3")
     digest = "not checked (size differs from the digest's)"
     if g and g["in_len"] == len(txt):
         if len(out) != g["out_len"] or hashlib.sha256(out).hexdigest() != g["out_sha256"]:
             raise SystemExit("chain digest check failed: output differs from the chained bytes.replace")
         digest = "sha256 equal to the chained bytes.replace"
-    t, te = statistics.median(dev_t), statistics.median(e2e_t)
+    t, te, launches, nsteps = res["staged"]
+    tp, tpe, lp, _ = res["per_pair"]
     return {"workload": f"{total / GiB:g} GiB tiled Zipf text x 128 entity pairs, Session.apply_batch",
             "gbs_sum_in_out": round(algo / t / 1e9, 2), "ms_per_chain": round(t * 1e3, 2),
-            "end_to_end_gbs": round((lens[0] + lens[-1]) / te / 1e9, 3), "end_to_end_ms": round(te * 1e3, 1),
-            "launches_per_chain": len(pairs), "final_len": lens[-1], "steps": len(dev_t), "check": digest,
+            "passes": launches, "end_to_end_gbs": round((lens[0] + lens[-1]) / te / 1e9, 3),
+            "end_to_end_ms": round(te * 1e3, 1),
+            "per_pair": {"passes": lp, "ms_per_chain": round(tp * 1e3, 2),
+                         "gbs_sum_in_out": round(algo / tp / 1e9, 2), "end_to_end_ms": round(tpe * 1e3, 1)},
+            "launches_per_chain": launches, "final_len": lens[-1], "steps": nsteps, "check": digest,
             "timer": "host clock around the synchronous call"}
 
 

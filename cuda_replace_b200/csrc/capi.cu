@@ -98,6 +98,13 @@ constexpr size_t kAllocQuantum = 2ull << 20;
 
 size_t round_up(size_t x, size_t q) { return (x + q - 1) / q * q; }
 
+// apply_batch runs runs of pairs proved independent in one pass each (multi-pattern stages)
+// unless the environment sets CUDA_REPLACE_STAGES=0 (every pair then gets its own pass).
+bool stages_enabled() {
+  const char* v = getenv("CUDA_REPLACE_STAGES");
+  return !(v && v[0] == '0');
+}
+
 // ------------------------------------------------------------------ page-locked host pool
 using crb::PinnedPool;
 PinnedPool& pinned_pool() { return crb::host_pinned_pool(); }
@@ -136,6 +143,9 @@ struct Session {
   unsigned long long* lens = nullptr;       // device: lengths along an apply_batch chain
   unsigned long long* lens_host = nullptr;  // page-locked mirror
   size_t lens_cap = 0;
+  crb::MultiTable* mtab = nullptr;          // device: pair tables of an apply_batch's stages
+  crb::MultiTable* mtab_host = nullptr;     // page-locked mirror
+  size_t mtab_cap = 0;
   cudaStream_t async_stream = nullptr;  // stream of the last cuda_replace_apply_device_async
   uint32_t async_epoch = 0;
   bool async_copy = false;          // the last async call copied its input (n < pattern length)
@@ -268,6 +278,8 @@ void session_free(Session* s) {
   if (s->ext_host) cudaFreeHost(s->ext_host);
   if (s->lens) cudaFree(s->lens);
   if (s->lens_host) cudaFreeHost(s->lens_host);
+  if (s->mtab) cudaFree(s->mtab);
+  if (s->mtab_host) cudaFreeHost(s->mtab_host);
   for (int k = 0; k < kUnifiedChunks; ++k) {
     if (s->ev_up[k]) cudaEventDestroy(s->ev_up[k]);
     if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
@@ -525,34 +537,70 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
   return kErrUnknown;
 }
 
-// apply_batch with the lengths chained on the device: one launch per pair and a single
-// read-back at the end, instead of a host round trip per pair. Used when every pair runs on
-// the super-tile kernel with inline pattern bytes and the worst-case lengths along the chain
-// fit in memory; returns kFallback when the caller must use one apply per pair.
+// apply_batch with the lengths chained on the device: one launch per stage (one pair, or a run
+// of pairs applied in one pass) and a single read-back at the end, instead of a host round trip
+// per pair. Used when every pair fits the super-tile kernel with inline pattern bytes and the
+// worst-case lengths along the chain fit in memory; returns kFallback when the caller must use
+// one apply per pair.
 int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
                         const int* rep_lens, int count, size_t* new_len) {
   if (count <= 0 || !pats || !reps || !pat_lens || !rep_lens) return kFallback;
-  std::vector<ReplaceParams> ps((size_t)count);
-  size_t b = s->len, maxb = s->len, tiles_max = 1, entries_max = 1;
   for (int k = 0; k < count; ++k) {
     const int pl = pat_lens[k], rl = rep_lens[k];
     if (pl < 1 || rl < 0 || pl > crb::kInlineMax || rl > crb::kInlineMax || !pats[k] || (rl && !reps[k])) return kFallback;
-    ReplaceParams& p = ps[(size_t)k];
+  }
+  // Stages: runs of pairs proved to give in one pass what they give one after the other
+  // (crb::plan_stages). The last pair runs alone, so query_prefix and the kept count after the
+  // batch describe the last pair's pass, as after the reference's per-pair loop (cu:2480-2519).
+  std::vector<int> stage_of((size_t)count);
+  int nst = count;
+  if (stages_enabled())
+    nst = crb::plan_stages(pats, pat_lens, reps, rep_lens, count, true, stage_of.data());
+  else
+    for (int k = 0; k < count; ++k) stage_of[(size_t)k] = k;
+  std::vector<ReplaceParams> ps((size_t)nst);
+  std::vector<crb::MultiTable> tabs;
+  std::vector<int> tab_of((size_t)nst, -1);
+  size_t b = s->len, maxb = s->len, tiles_max = 1, entries_max = 1;
+  for (int st = 0, k = 0; st < nst; ++st) {
+    int k1 = k;
+    while (k1 < count && stage_of[(size_t)k1] == st) ++k1;
+    ReplaceParams& p = ps[(size_t)st];
     memset(&p, 0, sizeof(p));
-    crb::prepare_pattern_fields(p, pats[k], (uint32_t)pl);
-    p.R = (uint32_t)rl;
-    p.nsub = crb::super_nsub(p.mode, p.L);
-    if (!p.nsub) return kFallback;
-    memcpy(p.pat, pats[k], (size_t)pl);
-    if (rl) memcpy(p.rep, reps[k], (size_t)rl);
+    size_t bnext;
+    if (k1 - k >= 2) {  // one pass over every pair of the stage
+      tabs.emplace_back();
+      crb::MultiTable& T = tabs.back();
+      crb::build_multi_table(T, pats + k, pat_lens + k, reps + k, rep_lens + k, k1 - k);
+      tab_of[(size_t)st] = (int)tabs.size() - 1;
+      p.mode = crb::kModeMulti;
+      p.L = T.Lmax;
+      p.R = 0;
+      p.agg_entries = 1;
+      p.multi_ratio = T.ratio;
+      p.nsub = crb::super_nsub(crb::kModeFree, 1);
+      bnext = (size_t)crb::multi_output_bound(T, b);
+      // the look-back sums sum(R - L) plus a bias per super-tile in 38-bit fields
+      if ((b / ((size_t)crb::kTile * p.nsub) + 2) * crb::kMultiBias + bnext >= (1ull << 37)) return kFallback;
+    } else {
+      const int pl = pat_lens[k], rl = rep_lens[k];
+      crb::prepare_pattern_fields(p, pats[k], (uint32_t)pl);
+      p.R = (uint32_t)rl;
+      p.nsub = crb::super_nsub(p.mode, p.L);
+      if (!p.nsub) return kFallback;
+      memcpy(p.pat, pats[k], (size_t)pl);
+      if (rl) memcpy(p.rep, reps[k], (size_t)rl);
+      bnext = output_bound(b, p.L, p.R);
+    }
     const size_t tb = (size_t)crb::kTile * p.nsub;
     const size_t tiles = (b + tb - 1) / tb;
     p.num_tiles = (uint32_t)(tiles ? tiles : 1);
     tiles_max = std::max(tiles_max, (size_t)p.num_tiles);
     entries_max = std::max(entries_max, (size_t)p.num_tiles * p.agg_entries);
-    b = output_bound(b, p.L, p.R);
-    if (b == SIZE_MAX) return kFallback;
+    if (bnext == SIZE_MAX) return kFallback;
+    b = bnext;
     maxb = std::max(maxb, b);
+    k = k1;
   }
   if (maxb > std::max<size_t>(4 * s->len, s->len + (1ull << 30))) return kFallback;
   cudaError_t e = dev_grow(&s->buf, &s->buf_cap, maxb ? maxb : 1, true, s->len, s->stream);
@@ -573,15 +621,34 @@ int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, c
     }
     s->lens_cap = cap;
   }
-  e = cudaStreamSynchronize(s->stream);  // the page-locked mirror may feed an earlier copy
+  if (tabs.size() > s->mtab_cap) {
+    if (s->mtab) cudaFree(s->mtab);
+    if (s->mtab_host) cudaFreeHost(s->mtab_host);
+    s->mtab = nullptr;
+    s->mtab_host = nullptr;
+    const size_t cap = tabs.size() + 8;
+    e = cudaMalloc(&s->mtab, cap * sizeof(crb::MultiTable));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->mtab_host, cap * sizeof(crb::MultiTable));
+    if (e != cudaSuccess) {
+      s->mtab_cap = 0;
+      return (int)e;
+    }
+    s->mtab_cap = cap;
+  }
+  e = cudaStreamSynchronize(s->stream);  // the page-locked mirrors may feed an earlier copy
   if (e != cudaSuccess) return (int)e;
   s->lens_host[0] = s->len;
   e = cudaMemcpyAsync(s->lens, s->lens_host, sizeof(unsigned long long), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess && !tabs.empty()) {
+    memcpy(s->mtab_host, tabs.data(), tabs.size() * sizeof(crb::MultiTable));
+    e = cudaMemcpyAsync(s->mtab, s->mtab_host, tabs.size() * sizeof(crb::MultiTable), cudaMemcpyHostToDevice,
+                        s->stream);
+  }
   if (e != cudaSuccess) return (int)e;
   uint8_t* bufs[2] = {s->buf, s->alt};
   const size_t cap = std::min(s->buf_cap, s->alt_cap);
   uint32_t first_epoch = 0;
-  for (int k = 0; k < count; ++k) {
+  for (int k = 0; k < nst; ++k) {
     ReplaceParams& p = ps[(size_t)k];
     p.in = bufs[k & 1];
     p.out = bufs[(k + 1) & 1];
@@ -596,28 +663,33 @@ int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, c
     p.rec = s->rec;
     p.epoch = next_epoch(s);
     if (k == 0) first_epoch = p.epoch;
-    e = crb::launch_replace_super(p, s->stream, nullptr);
+    if (tab_of[(size_t)k] >= 0) {
+      p.multi = s->mtab + tab_of[(size_t)k];
+      e = crb::launch_replace_multi(p, s->stream, nullptr);
+    } else {
+      e = crb::launch_replace_super(p, s->stream, nullptr);
+    }
     if (e != cudaSuccess) return (int)e;
     ++s->launches;
   }
-  e = cudaMemcpyAsync(s->lens_host, s->lens, ((size_t)count + 1) * sizeof(unsigned long long),
+  e = cudaMemcpyAsync(s->lens_host, s->lens, ((size_t)nst + 1) * sizeof(unsigned long long),
                       cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->res_host, s->res, sizeof(ApplyResult), cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return (int)e;
   const ApplyResult r = *s->res_host;
-  const uint32_t last_epoch = ps[(size_t)count - 1].epoch;
+  const uint32_t last_epoch = ps[(size_t)nst - 1].epoch;
   if ((r.error_epoch >= first_epoch && r.error_epoch <= last_epoch) ||
       (r.overflow_epoch >= first_epoch && r.overflow_epoch <= last_epoch))
     return kErrUnknown;
-  if (count & 1) swap_buffers(s);
-  s->len = (size_t)s->lens_host[count];
-  ReplaceParams q = ps[(size_t)count - 1];
-  q.n = s->lens_host[count - 1];
+  if (nst & 1) swap_buffers(s);
+  s->len = (size_t)s->lens_host[nst];
+  ReplaceParams q = ps[(size_t)nst - 1];  // a single pair (the last pair runs alone)
+  q.n = s->lens_host[nst - 1];
   q.n_dev = nullptr;
   q.len_out = nullptr;
-  s->q_kind = 2;
+  s->q_kind = q.mode == crb::kModeMulti ? 0 : 2;
   s->q_n = q.n;
   s->q_params = q;
   s->kept_last = r.kept;
@@ -736,6 +808,15 @@ void cache_give(Session* s) {
 }  // namespace
 
 CR_EXPORT const char* cuda_replace_version(void) { return "cuda_replace_b200 1.0 sm_100a single-pass look-back"; }
+
+CR_EXPORT int cuda_replace_plan_stages(const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+                                       const int* rep_lens, int count, int keep_last_alone, int* stage_of) {
+  if (count < 0 || (count > 0 && (!pats || !pat_lens || !reps || !rep_lens || !stage_of))) return -1;
+  for (int k = 0; k < count; ++k)
+    if (pat_lens[k] < 0 || rep_lens[k] < 0 || (pat_lens[k] && !pats[k]) || (rep_lens[k] && !reps[k])) return -1;
+  if (count == 0) return 0;
+  return crb::plan_stages(pats, pat_lens, reps, rep_lens, count, keep_last_alone != 0, stage_of);
+}
 
 CR_EXPORT void cuda_replace_host_copy(void* dst, const void* src, size_t n) {
   if (dst && src && n) crb::parallel_memcpy(dst, src, n);

@@ -984,6 +984,7 @@ constexpr int kMaxSub = 8;
 struct LayoutS {
   uint32_t in0, outb, masks, pat, rep, tab16, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
   uint32_t masks_set, srec_set, wtab_set, wrec_set, subrec_set;  // bytes of one set of per-super-tile tables
+  uint32_t mtab, tinfo, tinfo_set;  // kModeMulti: the stage's pair table; per-thread (D, last match end)
   uint32_t rs, inbytes;
   uint32_t wstage_words;  // padded staging words per warp (its 2 KiB of input may grow 3x)
   uint32_t wstage_cap;    // bytes one warp can stage (before the padding words)
@@ -1040,6 +1041,13 @@ __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_
     s.subrec = off;
     s.subrec_set = align_up_u32(nsub * L, 16);
     off += sets * s.subrec_set;
+  }
+  if (mode == kModeMulti) {
+    s.mtab = off;
+    off += align_up_u32((uint32_t)sizeof(MultiTable), 16);
+    s.tinfo = off;
+    s.tinfo_set = nsub * kThreads * 4u;
+    off += sets * s.tinfo_set;
   }
   s.total = off;
   return s;
@@ -1187,6 +1195,59 @@ __device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t 
     if (((ld_u32_unaligned(seg + b) ^ p4) & m4) == 0u) out |= 1ull << b;
   }
   return out;
+}
+
+// ---- kModeMulti helpers
+// Positions of the 64-byte segment at seg holding one of the stage's nfirst (1..4) distinct
+// first pattern bytes (`firsts`, one per byte lane): the four-bytes-per-operation byte test of
+// candidates_seg once per distinct byte, with the same conflict-free rotated reads.
+__device__ __forceinline__ uint64_t multi_first_mask(const uint8_t* seg, uint32_t firsts, uint32_t nfirst) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t rot = (lane >> 1) & 3u;
+  const uint4* v = reinterpret_cast<const uint4*>(seg);
+  const uint4 q0 = v[rot], q1 = v[(rot + 1u) & 3u], q2 = v[(rot + 2u) & 3u], q3 = v[(rot + 3u) & 3u];
+  uint64_t er = 0;
+  for (uint32_t k = 0; k < nfirst; ++k) {
+    const uint32_t rep = ((firsts >> (8u * k)) & 0xFFu) * 0x01010101u;
+    const uint32_t lo = eq_nibble(q0.x, rep) | (eq_nibble(q0.y, rep) << 4) | (eq_nibble(q0.z, rep) << 8) |
+                        (eq_nibble(q0.w, rep) << 12) | (eq_nibble(q1.x, rep) << 16) | (eq_nibble(q1.y, rep) << 20) |
+                        (eq_nibble(q1.z, rep) << 24) | (eq_nibble(q1.w, rep) << 28);
+    const uint32_t hi = eq_nibble(q2.x, rep) | (eq_nibble(q2.y, rep) << 4) | (eq_nibble(q2.z, rep) << 8) |
+                        (eq_nibble(q2.w, rep) << 12) | (eq_nibble(q3.x, rep) << 16) | (eq_nibble(q3.y, rep) << 20) |
+                        (eq_nibble(q3.z, rep) << 24) | (eq_nibble(q3.w, rep) << 28);
+    er |= ((uint64_t)hi << 32) | lo;  // chunk (rot + k) & 3 at bits 16k
+  }
+  const uint32_t sh = 16u * rot;
+  return sh ? ((er << sh) | (er >> (64u - sh))) : er;
+}
+
+// The pair of the stage whose pattern occurs at s (shared memory), or -1. room = input bytes
+// from s to the end of the buffer (a pattern must fit in them). No two patterns of a stage can
+// occur at one position (none is a prefix of another), so the first pair that matches is the
+// only one. One-byte patterns are found by their byte; longer ones through a hash of their
+// first two bytes, then compared.
+__device__ __forceinline__ int multi_identify(const MultiTable& T, const uint8_t* s, unsigned long long room) {
+  const uint32_t b0 = s[0];
+  uint32_t id = T.one[b0];
+  if (id) return (int)id - 1;
+  if (room < 2ull) return -1;
+  const uint32_t w = ld_u32_unaligned(s);
+  id = T.head[multi_hash(b0, (w >> 8) & 0xFFu)];
+  while (id) {
+    const uint32_t k = id - 1u;
+    const uint32_t L = T.L[k];
+    if ((unsigned long long)L <= room && ((w ^ T.p4[k]) & T.m4[k]) == 0u) {
+      bool ok = true;
+      for (uint32_t i = 4; i < L; ++i)
+        if (s[i] != T.pat[k][i]) {
+          ok = false;
+          break;
+        }
+      if (ok) return (int)k;
+    }
+    id = T.next[k];
+  }
+  return -1;
 }
 
 // Output staging: a word buffer with one padding word after every 32, so threads that
@@ -1792,12 +1853,14 @@ struct LoadRing {
   uint32_t ij;   // next sub-tile of the head phase
   uint32_t qh;   // head of the phase queue
   uint32_t nph;  // phases queued (at most kPhases)
+  uint32_t halo_b;  // pass-B loads include the halo (kModeMulti: a match's pattern is looked up again)
   uint32_t* q;   // the queue in shared memory: super-tile << 1 | kind (0: pass A, 1: pass B)
   static constexpr uint32_t kPhases = 4;
 
-  __device__ __forceinline__ void init(uint32_t* qs) {
+  __device__ __forceinline__ void init(uint32_t* qs, bool halo_in_b = false) {
     issued = consumed = 0;
     ij = qh = nph = 0;
+    halo_b = halo_in_b ? 1u : 0u;
     q = qs;
   }
   // Thread 0: queue the loads of one pass over super-tile t (kind 0: sub-tiles with their
@@ -1816,7 +1879,7 @@ struct LoadRing {
       const uint32_t m = subs_in_tile(t, S, n, nsub);
       const unsigned long long start = (unsigned long long)t * S + (unsigned long long)ij * kTile;
       const unsigned long long avail = n16 - start;
-      const uint32_t want = kind == 0 ? want_a : (uint32_t)kTile;
+      const uint32_t want = (kind == 0 || halo_b) ? want_a : (uint32_t)kTile;
       const uint32_t bytes = avail < want ? (uint32_t)avail : want;
       const uint32_t b = issued % kNBuf;
       // no proxy fence: the buffer's earlier contents were only read, and every read of them
@@ -2013,6 +2076,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ uint32_t s_sub_lco[2 * kMaxSub];
   __shared__ uint32_t s_wcnt[2 * kMaxSub * kWarps];   // kModeFree: kept count per (sub-tile, warp)
   __shared__ uint32_t s_wcend[2 * kMaxSub * kWarps];  // kModeFree: max cover end per (sub-tile, warp)
+  __shared__ int s_wd[2 * kMaxSub * kWarps];          // kModeMulti: sum of R - L per (sub-tile, warp)
   __shared__ unsigned long long s_frcnt[2];          // kModeFree: super-tile function (count, local carry-out)
   __shared__ long long s_frlco[2];
   __shared__ uint32_t s_supc[2][32], s_supx[2][32];  // kModeSmall: super-tile table over carries
@@ -2024,11 +2088,15 @@ __global__ void __launch_bounds__(kThreads, 3)
   unsigned int* const sched = SEG ? sl.sched : &pk.res->tile_counter;  // claim counter, then finished CTAs
   const uint32_t nsub = SEG ? sl.nsub : pk.nsub;
   const LayoutS lay =
-      SEG ? make_layout_s(MODE, sl.Lmax, sl.Rmax, nsub, 3u) : make_layout_s(MODE, pk.L, pk.R, nsub, 0u, 2u);
+      SEG ? make_layout_s(MODE, sl.Lmax, sl.Rmax, nsub, 3u)
+          : make_layout_s(MODE, pk.L, pk.R, nsub, MODE == kModeMulti ? pk.multi_ratio : 0u, 2u);
   uint8_t* ps = smem + lay.pat;
   uint8_t* rs = smem + lay.rep;
   uint8_t* ob = smem + lay.outb;
   uint64_t* masks = reinterpret_cast<uint64_t*>(smem + lay.masks);
+  // kModeMulti follows the free-mode paths (every occurrence kept), with per-pair lengths
+  constexpr bool kFreeLike = MODE == kModeFree || MODE == kModeMulti;
+  const MultiTable& MT = *reinterpret_cast<const MultiTable*>(smem + lay.mtab);
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t sb = tid * kSeg;
   const unsigned long long S = (unsigned long long)nsub * kTile;
@@ -2061,6 +2129,11 @@ __global__ void __launch_bounds__(kThreads, 3)
       uint8_t* t16 = smem + lay.tab16;
       for (uint32_t i = tid; i < R * 16u; i += kThreads) t16[i] = rsrc[((i >> 4) + (i & 15u)) % R];
     }
+    if constexpr (MODE == kModeMulti) {  // the stage's pair table
+      const uint4* src = reinterpret_cast<const uint4*>(p.multi);
+      uint4* dst = reinterpret_cast<uint4*>(smem + lay.mtab);
+      for (uint32_t i = tid; i < (uint32_t)(sizeof(MultiTable) / 16u); i += kThreads) dst[i] = src[i];
+    }
   };
   if (!SEG) {
     setup_job();
@@ -2075,7 +2148,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 
   // ---- load ring: thread 0 queues the loads of each pass in the order they are consumed
   LoadRing ring;
-  ring.init(s_phq);
+  ring.init(s_phq, MODE == kModeMulti);
 
   // pass A of super-tile t and its function (published as an aggregate record); tables in set `set`
   auto tile_front = [&](const uint32_t t, const uint32_t set) {
@@ -2092,13 +2165,20 @@ __global__ void __launch_bounds__(kThreads, 3)
     // ================= pass A: candidates and per-warp functions of every sub-tile
     bool run_try = run_pat;  // re-armed for every super-tile
     // bounds: candidates p in [block_before, lim); a super-tile inside both needs no masking
-    const unsigned long long lim = (n_all >= L) ? min(n_all - L + 1, n) : 0ull;  // candidates p < lim
+    // (kModeMulti: p < n here; each pattern's own length is checked against n_all when found)
+    const unsigned long long lim =
+        MODE == kModeMulti ? n : ((n_all >= L) ? min(n_all - L + 1, n) : 0ull);  // candidates p < lim
     const bool edge = tstart < p.block_before || tstart + (unsigned long long)m * kTile > lim;
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
-      bool uni;
-      uint64_t mask = candidates_seg(tb + sb, p.p4, p.m4, L, run_try, &uni);
+      bool uni = false;
+      uint64_t mask;
+      if constexpr (MODE == kModeMulti) {
+        mask = multi_first_mask(tb + sb, MT.firsts, MT.nfirst);
+      } else {
+        mask = candidates_seg(tb + sb, p.p4, p.m4, L, run_try, &uni);
+      }
       run_try = uni;  // keep testing while the text is runs of b0
       const unsigned long long sub0 = tstart + (unsigned long long)j * kTile;
       if (edge && (sub0 < p.block_before || sub0 + kTile > lim)) {
@@ -2113,6 +2193,35 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         mask &= low_bits(hi) & ~low_bits(lo);
       }
+      if constexpr (MODE == kModeMulti) {
+        // each position holding a first pattern byte: which pattern occurs there, if any; every
+        // occurrence is kept. Per thread: D = sum of R - L, and where its last match ends.
+        uint64_t kept = 0;
+        int dsum = 0;
+        uint32_t lastend = 0;
+        while (mask) {
+          const uint32_t b = (uint32_t)(__ffsll((long long)mask) - 1);
+          mask &= mask - 1ull;
+          const int k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
+          if (k >= 0) {
+            kept |= 1ull << b;
+            dsum += (int)MT.R[k] - (int)MT.L[k];
+            lastend = b + MT.L[k];
+          }
+        }
+        mask = kept;
+        masks_s[j * kThreads + tid] = mask;
+        reinterpret_cast<uint32_t*>(smem + lay.tinfo + set * lay.tinfo_set)[j * kThreads + tid] =
+            ((uint32_t)dsum & 0xFFFFu) | (lastend << 16);
+        const uint32_t cnt = __reduce_add_sync(0xffffffffu, (uint32_t)__popcll(mask));
+        const int wd = __reduce_add_sync(0xffffffffu, dsum);
+        const uint32_t cend = __reduce_max_sync(0xffffffffu, mask ? sb + lastend : 0u);
+        if (lane == 0) {
+          wcnt_s[j * kWarps + warp] = cnt;
+          s_wd[set * (kMaxSub * kWarps) + j * kWarps + warp] = wd;
+          wcend_s[j * kWarps + warp] = cend;
+        }
+      } else {
       if (L > 4) mask = verify_tail(mask, tb + sb, ps, L);
       masks_s[j * kThreads + tid] = mask;
       if (MODE == kModeFree) {
@@ -2154,6 +2263,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           }
         }
       }
+      }  // not kModeMulti
       __syncthreads();
       ring.release();
       if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
@@ -2161,7 +2271,7 @@ __global__ void __launch_bounds__(kThreads, 3)
 
     // ================= fold the sub-tiles into the super-tile function
     // (warp 1, so that warp 0 can start the previous super-tile's look-back at the same time)
-    const bool use_rec = MODE == kModeFree || L <= 4u;
+    const bool use_rec = kFreeLike || L <= 4u;
     const uint32_t tag = p.epoch & 0xFFFFFFu;
     unsigned long long fr_cnt = 0;  // kModeFree: lane 0 of warp 1
     long long fr_lco = 0;
@@ -2176,13 +2286,14 @@ __global__ void __launch_bounds__(kThreads, 3)
     const bool whole = !SEG && m == nsub && nsub * kWarps <= 32u && tstart + S <= n && L <= 64u &&
                        (R == 0u || rep_table);
     uint32_t noin = 0;
-    if (MODE == kModeFree) {
+    if (kFreeLike) {
       if (warp == 1) {
         // lane r stands for warp region r % 8 of sub-tile j0 + r / 8 (groups of 8 lanes)
         const uint32_t wr = lane & 7u;
         bool ok = whole;   // every region covered end to end (whole: m <= 4, one round)
         bool tin = whole;  // every region covered end to end or free of kept starts
         uint32_t cnt_sum = 0;
+        int dsum = 0;      // kModeMulti: sum of R - L over the super-tile's matches
         long long lco_max = LLONG_MIN;
         for (uint32_t j0 = 0; j0 < m; j0 += 4u) {
           const uint32_t jr = j0 + (lane >> 3);
@@ -2202,6 +2313,8 @@ __global__ void __launch_bounds__(kThreads, 3)
           const uint32_t lco = gmax > (uint32_t)kTile ? gmax - (uint32_t)kTile : 0u;  // reach past the sub-tile
           if (act && wr == 0) sublco_s[jr] = lco;
           cnt_sum += __reduce_add_sync(0xffffffffu, wc);
+          if (MODE == kModeMulti)
+            dsum += __reduce_add_sync(0xffffffffu, act ? s_wd[set * (kMaxSub * kWarps) + jr * kWarps + wr] : 0);
           // the super-tile's reach: max over sub-tiles of their reach, less the sub-tiles after them
           const long long v = act ? (long long)lco - (long long)(m - 1u - jr) * kTile : LLONG_MIN;
           lco_max = v > lco_max ? v : lco_max;
@@ -2214,7 +2327,8 @@ __global__ void __launch_bounds__(kThreads, 3)
             uint32_t wcov = covs > wlo ? covs - wlo : 0u;
             wcov = wcov < 2048u ? wcov : 2048u;
             const uint32_t over = ce > wlo + 2048u ? ce - (wlo + 2048u) : 0u;
-            const bool full = 2048u - wcov - wc * L + over == 0u;
+            // (kModeMulti: the replacements differ, so no region is a run of one replacement)
+            const bool full = MODE != kModeMulti && 2048u - wcov - wc * L + over == 0u;
             ok = __all_sync(0xffffffffu, !act || full);
             tin = __all_sync(0xffffffffu, !act || full || wc == 0u);
           }
@@ -2224,7 +2338,8 @@ __global__ void __launch_bounds__(kThreads, 3)
           const long long o = __shfl_xor_sync(0xffffffffu, lco_max, d);
           lco_max = o > lco_max ? o : lco_max;
         }
-        fr_cnt = cnt_sum;
+        // kModeMulti: the look-back sums sum(R - L) + kMultiBias per super-tile (a payload >= 0)
+        fr_cnt = MODE == kModeMulti ? (unsigned long long)((long long)dsum + (long long)kMultiBias) : cnt_sum;
         fr_lco = lco_max;
         noin = ok ? 1u : (tin ? 2u : 0u);
         if (lane == 0 && t > 0)
@@ -2289,7 +2404,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
 
-    if (MODE == kModeFree) {
+    if (kFreeLike) {
       if (tid == 32u) {
         s_frcnt[set] = fr_cnt;
         s_frlco[set] = fr_lco;
@@ -2327,7 +2442,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     uint8_t* const wtab_b = smem + lay.wtab + set * lay.wtab_set;
     uint8_t* const wrec_b = smem + lay.wrec + set * lay.wrec_set;
     uint8_t* const subrec_b = smem + lay.subrec + set * lay.subrec_set;
-    const bool use_rec = MODE == kModeFree || L <= 4u;
+    const bool use_rec = kFreeLike || L <= 4u;
     const uint32_t tag = p.epoch & 0xFFFFFFu;
     // ================= look back, publish the inclusive prefix
     if (warp == 0) {
@@ -2335,7 +2450,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       uint32_t c = carry0;
       bool ok = true;
       if (t > 0) {
-        if (MODE == kModeFree)
+        if (kFreeLike)
           ok = lookback_free_rec(p, t, S, &K, &c, carry0);
         else if (L == 2u)
           ok = lookback_small_rec<2>(p, t, &K, &c, carry0);
@@ -2353,7 +2468,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       unsigned long long Kin;
       uint32_t cout;
-      if (MODE == kModeFree) {
+      if (kFreeLike) {
         const unsigned long long fcnt = s_frcnt[set];
         const long long flco = s_frlco[set];
         const long long sh = (long long)c - (long long)m * kTile;  // span of this super-tile
@@ -2387,8 +2502,12 @@ __global__ void __launch_bounds__(kThreads, 3)
     const long long delta = (long long)R - (long long)L;
     // output position in out[]: the output range starts len_bias bytes in, and the carry0
     // leading bytes covered by a match kept before this buffer are not emitted here
-    unsigned long long O = p.len_bias + (unsigned long long)((long long)(tstart + cin) - (long long)carry0 +
-                                                             (long long)kexcl * delta);
+    // (kModeMulti: the look-back prefix is sum(R - L) over the earlier matches plus kMultiBias per
+    // earlier super-tile)
+    const long long dprefix = MODE == kModeMulti ? (long long)kexcl - (long long)t * (long long)kMultiBias
+                                                 : (long long)kexcl * delta;
+    unsigned long long O =
+        p.len_bias + (unsigned long long)((long long)(tstart + cin) - (long long)carry0 + dprefix);
     const bool failed = s_fail != 0;
 
     // ================= pass B, table-driven: every warp region of this whole super-tile is a run of
@@ -2421,12 +2540,12 @@ __global__ void __launch_bounds__(kThreads, 3)
     } else if (pbm == 2u) {
       const uint32_t jr = lane >> 3, wr = lane & 7u;
       uint32_t wc = 0, x0 = 0, olen_r = 0, we = 0;
-      if (MODE == kModeFree && jr < m) {
+      if (kFreeLike && jr < m) {
         wc = wcnt_s[lane];  // index jr * kWarps + wr
         we = wcend_s[lane];
       }
       uint32_t pre = we;  // kModeFree: max cover end of the earlier regions of the same sub-tile
-      if (MODE == kModeFree) {
+      if (kFreeLike) {
 #pragma unroll
         for (int d = 1; d < 8; d <<= 1) {
           const uint32_t o = __shfl_up_sync(0xffffffffu, pre, d, 8);
@@ -2435,7 +2554,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         pre = __shfl_up_sync(0xffffffffu, pre, 1, 8);
       }
       if (jr < m) {
-        if (MODE == kModeFree) {
+        if (kFreeLike) {
           // carry into sub-tile jr: cin, then the previous sub-tile's reach (L <= 64, so a cover
           // never spans a whole sub-tile)
           const uint32_t csj = jr == 0 ? cin : sublco_s[jr - 1];
@@ -2507,7 +2626,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       uint32_t x_in = 0, cnt, wolen = 0;
       uint64_t kept;
       uint32_t csub_in = 0, covs_l = 0, ewc = 0, ewcov = 0;  // kModeFree: kept for x_in and the warp paths
-      if (MODE == kModeFree) {
+      if (kFreeLike) {
         const uint32_t wc = lane < 8u ? wcnt_s[j * kWarps + lane] : 0u;
         const uint32_t we = lane < 8u ? wcend_s[j * kWarps + lane] : 0u;
         const uint32_t pre = lanes8_excl_max(we);  // max cover end of the earlier warps
@@ -2515,7 +2634,11 @@ __global__ void __launch_bounds__(kThreads, 3)
         const uint32_t wlo = lane * 2048u, whi = wlo + 2048u;
         const uint32_t wcov = covs > wlo ? covs - wlo : 0u;
         const uint32_t over = we > whi ? we - whi : 0u;
-        wolen = wbytes - (wcov < wbytes ? wcov : wbytes) - wc * L + over + wc * R;
+        // the region's matches change its length by wc * (R - L), or (kModeMulti) by their sum of R - L
+        const uint32_t grow = MODE == kModeMulti
+                                  ? (lane < 8u ? (uint32_t)s_wd[set * (kMaxSub * kWarps) + j * kWarps + lane] : 0u)
+                                  : wc * R - wc * L;
+        wolen = wbytes - (wcov < wbytes ? wcov : wbytes) + over + grow;
         csub_in = csub;
         covs_l = covs;
         ewc = wc;
@@ -2563,7 +2686,7 @@ __global__ void __launch_bounds__(kThreads, 3)
           const bool table_only = stage0 && (wcw == 0u || wlw == 0u || (rep_table && wlw == wcw * R));
           if (table_only) {
             // the last kept start, from the tables (also when nothing is written below)
-            if (MODE == kModeFree) {
+            if (kFreeLike) {
               if (mask) last_abs = (long long)(gseg + (63u - (uint32_t)__clzll((long long)mask)));
             } else if (wcw != 0u && lane == 0) {
               // a region with no literal byte: its kept starts are cw, cw + L, ... (the block
@@ -2583,8 +2706,19 @@ __global__ void __launch_bounds__(kThreads, 3)
           }
         }
       }
+      uint32_t tinf = 0;  // kModeMulti: this thread's (sum of R - L, last match end)
       if (!done) {
-      if (MODE == kModeFree) {
+      if constexpr (MODE == kModeMulti) {
+        // only the previous segment's last match (or the sub-tile carry) can reach here (L <= 32)
+        const uint32_t* tinfo = reinterpret_cast<const uint32_t*>(smem + lay.tinfo + set * lay.tinfo_set);
+        tinf = tinfo[j * kThreads + tid];
+        uint32_t cov = tid == 0 ? csub_in : 0u;
+        if (tid > 0) {
+          const uint32_t e = tinfo[j * kThreads + tid - 1] >> 16;
+          if (e > 64u) cov = e - 64u;
+        }
+        x_in = cov;
+      } else if (MODE == kModeFree) {
         if (L <= 64u) {
           // only the previous segment's last match (or the sub-tile carry) can reach here
           uint32_t cov = tid == 0 ? csub_in : 0u;
@@ -2621,13 +2755,23 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       const uint32_t V = gseg >= n ? 0u : ((n - gseg) < 64ull ? (uint32_t)(n - gseg) : 64u);
       uint32_t covered = x_in < V ? x_in : V;
-      if (cnt) {
-        const uint32_t lastk = 63u - (uint32_t)__clzll((long long)kept);
-        const uint32_t over = (lastk + L > V) ? lastk + L - V : 0u;
-        covered += cnt * L - over;
-        last_abs = (long long)(gseg + lastk);
+      uint32_t olen;
+      if constexpr (MODE == kModeMulti) {
+        // literal bytes V - x_in - sum(L) + (what the last match covers past V), plus sum(R)
+        const int dthr = (int)(int16_t)(tinf & 0xFFFFu);
+        const uint32_t le = tinf >> 16;
+        const uint32_t over = (cnt && le > V) ? le - V : 0u;
+        if (cnt) last_abs = (long long)(gseg + (63u - (uint32_t)__clzll((long long)kept)));
+        olen = (uint32_t)((int)(V - covered + over) + dthr);
+      } else {
+        if (cnt) {
+          const uint32_t lastk = 63u - (uint32_t)__clzll((long long)kept);
+          const uint32_t over = (lastk + L > V) ? lastk + L - V : 0u;
+          covered += cnt * L - over;
+          last_abs = (long long)(gseg + lastk);
+        }
+        olen = V - covered + cnt * R;
       }
-      const uint32_t olen = V - covered + cnt * R;
       uint32_t toff = warp_incl_scan(olen, OpSum());
       const uint32_t wtot = __shfl_sync(0xffffffffu, toff, 31);
       toff -= olen;  // exclusive offset inside the warp region
@@ -2654,12 +2798,22 @@ __global__ void __launch_bounds__(kThreads, 3)
       // 0-7 of every warp hold the eight lengths, so the choice is the same in every warp.
       const bool warp_stage = __reduce_max_sync(0xffffffffu, lane < 8u ? wolen : 0u) + 15u <= lay.wstage_cap;
       if (!fits && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
+      // kModeMulti: the warp's own sum of its threads' lengths must equal the length its slot was
+      // given from the pass-A sums, or it would write over its neighbour; a mismatch (which the
+      // arithmetic rules out) is reported as an error and the warp writes nothing. The same in
+      // every lane of the warp; the branches below keep their block-uniform choice regardless.
+      bool len_ok = true;
+      if (MODE == kModeMulti) {
+        len_ok = __shfl_sync(0xffffffffu, wolen, warp) == wtot;
+        if (!len_ok && lane == 0) set_error(p);
+      }
       // warp output mode: no kept match in the warp (a copy of its input), or no literal byte
       // (a run of replacements), or mixed
       const uint32_t notlit = __ballot_sync(0xffffffffu, cnt != 0u || (lane > 0u && x_in != 0u));
       const uint32_t notrep = __ballot_sync(0xffffffffu, olen != cnt * R);
       if (fits && !failed && warp_stage && wtot != 0u && (notlit == 0u || (notrep == 0u && rep_table))) {
-        if (notlit == 0u) {
+        if (!len_ok) {
+        } else if (notlit == 0u) {
           // ---- LITERAL: output = input bytes [warp start + x0, ...)
           warp_emit_literal(p.out, tb, O + wbase, wtot, warp * 2048u + __shfl_sync(0xffffffffu, x_in, 0));
         } else {
@@ -2668,6 +2822,7 @@ __global__ void __launch_bounds__(kThreads, 3)
                             wtot);
         }
       } else if (fits && !failed && warp_stage) {
+        if (len_ok) {
         uint32_t W[17];
         load_seg_words(tb + sb, W);
         // ---- this warp's output: assemble in its padded staging area, then copy out
@@ -2706,6 +2861,13 @@ __global__ void __launch_bounds__(kThreads, 3)
             if (nk > V) nk = V;
             if (nk > pos) emit_literal(e, src + pos, nk - pos);
             if (nk >= V) break;
+            if constexpr (MODE == kModeMulti) {  // this match's own replacement
+              const int k = multi_identify(MT, src + nk, n_all - (gseg + nk));
+              if (k < 0) break;  // cannot happen: pass A found this pattern here
+              emit_literal(e, MT.rep[k], MT.R[k]);
+              pos = nk + MT.L[k];
+              continue;
+            }
             uint32_t r = 1;  // kept starts nk, nk+L, ... with nothing literal between them
             if (L < 64u) {
               const uint64_t holes = p.stride_mask & ~(kept >> nk);
@@ -2749,6 +2911,7 @@ __global__ void __launch_bounds__(kThreads, 3)
             p.out[b] = sbytes[stg_pad(sbi >> 2) * 4u + (sbi & 3u)];
           }
         }
+        }  // len_ok
       } else if (fits && !failed) {
         // very large expansions: windows of the sub-tile output, byte by byte (the windows
         // share the staging area with the warps' own staging, which the block barrier at the
@@ -2771,6 +2934,14 @@ __global__ void __launch_bounds__(kThreads, 3)
               copy_clip(obw, o, src + pos, nk - pos, w0, w1);
               o += nk - pos;
               if (nk >= V) break;
+              if constexpr (MODE == kModeMulti) {  // this match's own replacement
+                const int k = multi_identify(MT, src + nk, n_all - (gseg + nk));
+                if (k < 0) break;  // cannot happen: pass A found this pattern here
+                copy_clip(obw, o, MT.rep[k], MT.R[k], w0, w1);
+                o += MT.R[k];
+                pos = nk + MT.L[k];
+                continue;
+              }
               copy_clip(obw, o, rs, R, w0, w1);
               o += R;
               pos = nk + L;
@@ -2815,9 +2986,10 @@ __global__ void __launch_bounds__(kThreads, 3)
           atomicMax(&p.res->last_tagged, ((unsigned long long)p.epoch << 40) | (unsigned long long)(lastt + 1));
         if (t == NT - 1) {
           p.res->out_len = O - p.len_bias;
-          p.res->kept = __ldcg(&p.incl[t].kept);
+          // (kModeMulti: the look-back sums are not match counts; no count is reported)
+          p.res->kept = MODE == kModeMulti ? 0ull : __ldcg(&p.incl[t].kept);
           if (p.len_out) *p.len_out = O;
-          if (p.carry_out) {
+          if (MODE != kModeMulti && p.carry_out) {
             // coverage past the output range n: by the last kept match, or by the carry into
             // this super-tile when no match starts in it
             unsigned long long e = tstart + cin;
@@ -3296,6 +3468,174 @@ cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const 
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   empty_pattern_kernel<<<(unsigned)blocks, 256, 0, st>>>(in, n, rep_dev, R, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- multi-pattern stages
+namespace {
+
+bool bytes_equal(const uint8_t* a, const uint8_t* b, uint32_t n) { return n == 0 || std::memcmp(a, b, n) == 0; }
+
+// Can an occurrence of a and an occurrence of b (different pairs, or the same pattern at two
+// positions) overlap in some text? Yes when they are equal (two pairs with one pattern), when
+// one lies inside the other, or when a proper suffix of one is a proper prefix of the other
+// (for a == b alone: a proper border).
+bool may_overlap(const uint8_t* a, uint32_t La, const uint8_t* b, uint32_t Lb, bool same_pair) {
+  if (!same_pair && La == Lb && bytes_equal(a, b, La)) return true;
+  if (!same_pair) {
+    if (Lb < La)
+      for (uint32_t o = 0; o + Lb <= La; ++o)
+        if (bytes_equal(a + o, b, Lb)) return true;
+    if (La < Lb)
+      for (uint32_t o = 0; o + La <= Lb; ++o)
+        if (bytes_equal(b + o, a, La)) return true;
+  }
+  const uint32_t m = La < Lb ? La : Lb;
+  for (uint32_t k = 1; k < m; ++k) {
+    if (bytes_equal(a + (La - k), b, k)) return true;
+    if (bytes_equal(b + (Lb - k), a, k)) return true;
+  }
+  return false;
+}
+
+// Can replacement r (of an earlier pair), with whatever bytes surround it, form an occurrence of
+// pattern p (of a later pair) that overlaps it? An occurrence that includes no byte of r lay
+// entirely before or after it, so it was there before the replacement; one that overlaps r
+// must agree with r wherever they overlap. An empty r joins its two neighbours, which any
+// pattern of two bytes or more may straddle.
+bool may_create(const uint8_t* r, uint32_t R, const uint8_t* p, uint32_t L) {
+  if (R == 0) return L >= 2;
+  for (int d = -(int)L + 1; d < (int)R; ++d) {  // p starts d bytes after r starts
+    bool ok = true;
+    for (uint32_t k = 0; k < L && ok; ++k) {
+      const int i = d + (int)k;
+      if (i >= 0 && i < (int)R && p[k] != r[i]) ok = false;
+    }
+    if (ok) return true;
+  }
+  return false;
+}
+
+bool multi_eligible(const uint8_t* pat, int L, int R) {
+  return L >= 1 && L <= (int)kMultiMaxL && R >= 0 && R <= (int)kMultiMaxR && pat != nullptr &&
+         !may_overlap(pat, (uint32_t)L, pat, (uint32_t)L, true);
+}
+
+}  // namespace
+
+int plan_stages(const uint8_t* const* pats, const int* pat_lens, const uint8_t* const* reps,
+                const int* rep_lens, int count, bool keep_last_alone, int* stage_of) {
+  int stage = -1, first = 0;  // current stage and its first pair
+  uint32_t firsts[kMultiMaxFirst];
+  uint32_t nfirst = 0;
+  bool open = false;  // the current stage can take more pairs
+  for (int k = 0; k < count; ++k) {
+    const int L = pat_lens[k], R = rep_lens[k];
+    const bool elig = multi_eligible(pats[k], L, R) && !(keep_last_alone && k == count - 1);
+    bool join = open && elig && (k - first) < (int)kMultiMaxPairs;
+    if (join) {
+      const uint32_t b0 = pats[k][0];
+      bool known = false;
+      for (uint32_t f = 0; f < nfirst; ++f) known = known || firsts[f] == b0;
+      if (!known && nfirst == kMultiMaxFirst) join = false;
+      for (int i = first; i < k && join; ++i) {
+        if (may_overlap(pats[i], (uint32_t)pat_lens[i], pats[k], (uint32_t)L, false) ||
+            may_create(reps[i], (uint32_t)rep_lens[i], pats[k], (uint32_t)L))
+          join = false;
+      }
+      if (join && !known) firsts[nfirst++] = b0;
+    }
+    if (!join) {
+      ++stage;
+      first = k;
+      open = elig;
+      nfirst = 0;
+      if (elig) firsts[nfirst++] = pats[k][0];
+    }
+    stage_of[k] = stage;
+  }
+  return stage + 1;
+}
+
+void build_multi_table(MultiTable& T, const uint8_t* const* pats, const int* pat_lens, const uint8_t* const* reps,
+                       const int* rep_lens, int count) {
+  std::memset(&T, 0, sizeof(T));
+  T.npairs = (uint32_t)count;
+  T.Lmin = ~0u;
+  uint32_t ratio = 1;
+  for (int k = 0; k < count; ++k) {
+    const uint32_t L = (uint32_t)pat_lens[k], R = (uint32_t)rep_lens[k];
+    T.L[k] = (uint8_t)L;
+    T.R[k] = (uint8_t)R;
+    T.Lmin = L < T.Lmin ? L : T.Lmin;
+    T.Lmax = L > T.Lmax ? L : T.Lmax;
+    std::memcpy(T.pat[k], pats[k], L);
+    if (R) std::memcpy(T.rep[k], reps[k], R);
+    for (uint32_t i = 0; i < 4 && i < L; ++i) {
+      T.p4[k] |= (uint32_t)pats[k][i] << (8 * i);
+      T.m4[k] |= 0xFFu << (8 * i);
+    }
+    const uint32_t b0 = pats[k][0];
+    bool known = false;
+    for (uint32_t f = 0; f < T.nfirst; ++f) known = known || ((T.firsts >> (8 * f)) & 0xFFu) == b0;
+    if (!known) T.firsts |= b0 << (8 * T.nfirst++);
+    if (L == 1) {
+      T.one[b0] = (uint8_t)(k + 1);
+    } else {  // chained in pair order behind the hash of the first two bytes
+      const uint32_t h = multi_hash(b0, pats[k][1]);
+      if (!T.head[h]) {
+        T.head[h] = (uint8_t)(k + 1);
+      } else {
+        uint32_t c = T.head[h] - 1u;
+        while (T.next[c]) c = T.next[c] - 1u;
+        T.next[c] = (uint8_t)(k + 1);
+      }
+    }
+    const uint32_t r = R > L ? (R + L - 1) / L : 1u;
+    ratio = r > ratio ? r : ratio;
+  }
+  T.ratio = ratio < 3u ? ratio : 3u;
+}
+
+unsigned long long multi_output_bound(const MultiTable& T, unsigned long long n) {
+  unsigned __int128 grow = 0;
+  for (uint32_t k = 0; k < T.npairs; ++k)
+    if (T.R[k] > T.L[k]) {
+      const unsigned __int128 g = (unsigned __int128)(n / T.L[k]) * (T.R[k] - T.L[k]);
+      grow = g > grow ? g : grow;
+    }
+  const unsigned __int128 b = (unsigned __int128)n + grow;
+  return b > (unsigned __int128)~0ull ? ~0ull : (unsigned long long)b;
+}
+
+cudaError_t launch_replace_multi(const ReplaceParams& p, cudaStream_t st, int* grid_out) {
+  if (p.mode != kModeMulti || !p.multi || !p.nsub || p.hold || p.carry_out || p.carry0 || p.carry0_dev ||
+      p.L > kMultiMaxL)
+    return cudaErrorInvalidValue;
+  static std::mutex mu;
+  static unsigned long long attr_dev_mask = 0;
+  const uint32_t smem = make_layout_s(kModeMulti, p.L, p.R, p.nsub, p.multi_ratio, 2u).total;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!(attr_dev_mask & (1ull << (dev & 63)))) {
+      cudaError_t e = cudaFuncSetAttribute(replace_super_kernel<kModeMulti, false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      if (e != cudaSuccess) return e;
+      attr_dev_mask |= 1ull << (dev & 63);
+    }
+  }
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, replace_super_kernel<kModeMulti, false>,
+                                                                kThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  long long grid = (long long)per_sm * device_sm_count();
+  if (grid > (long long)p.num_tiles) grid = p.num_tiles;
+  if (grid < 1) grid = 1;
+  replace_super_kernel<kModeMulti, false><<<(unsigned)grid, kThreads, smem, st>>>(p, SegLaunch{});
+  if (grid_out) *grid_out = (int)grid;
   return cudaGetLastError();
 }
 

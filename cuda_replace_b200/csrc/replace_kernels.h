@@ -31,7 +31,42 @@ constexpr uint32_t kMaxLen = 8192;          // longest pattern / replacement (CU
 //              covered. A tile's function is carry_out(c) = max(c - kTile, lco).
 //  kModeSmall: P has a border and L <= 64: the tile function is a table over c in [0, L).
 //  kModeLarge: P has a border and L > 64: same table, built without the warp level.
-enum CarryMode : uint32_t { kModeFree = 0, kModeSmall = 1, kModeLarge = 2 };
+//  kModeMulti: several (pattern, replacement) pairs applied in one pass, with the result of
+//              applying them one after the other (a "stage" of an apply_batch chain; see
+//              MultiTable). No two occurrences of the stage's patterns can overlap, so, as in
+//              kModeFree, every occurrence is kept and the carry only tells which leading bytes
+//              are covered; the output offset advances by R_i - L_i per occurrence of pair i.
+enum CarryMode : uint32_t { kModeFree = 0, kModeSmall = 1, kModeLarge = 2, kModeMulti = 3 };
+
+// ---- Multi-pattern stages. A run of consecutive pairs of a chain is applied in ONE pass when
+// the host has proved (plan_stages) that applying them one after the other gives the same
+// bytes as replacing every occurrence of every pattern of the run in the run's input at once:
+// no occurrence of one pattern can overlap an occurrence of another (or of itself), and no
+// replacement of an earlier pair can form, with the bytes around it, an occurrence of a later
+// pattern. The stage's pairs live in a table in device memory, staged into shared memory.
+constexpr uint32_t kMultiMaxPairs = 32;
+constexpr uint32_t kMultiMaxL = 32;
+constexpr uint32_t kMultiMaxR = 64;
+constexpr uint32_t kMultiMaxFirst = 4;             // distinct first pattern bytes of a stage
+constexpr unsigned long long kMultiBias = 65536;   // look-back payload bias per super-tile (>= its bytes)
+
+struct MultiTable {
+  uint32_t npairs, nfirst, Lmin, Lmax;
+  uint32_t firsts;                     // the nfirst distinct first bytes, one per byte lane
+  uint32_t ratio;                      // output staging per input byte (1..3)
+  uint32_t pad[2];
+  uint32_t p4[kMultiMaxPairs], m4[kMultiMaxPairs];  // first min(L, 4) bytes and their mask
+  uint8_t L[kMultiMaxPairs], R[kMultiMaxPairs];
+  uint8_t next[kMultiMaxPairs];        // hash chain: next pair + 1 (0 = end)
+  uint8_t pad2[kMultiMaxPairs];
+  uint8_t one[256];                    // byte -> pair + 1 of a one-byte pattern (0 = none)
+  uint8_t head[256];                   // hash of the first two bytes -> first pair + 1
+  uint8_t pat[kMultiMaxPairs][kMultiMaxL];
+  uint8_t rep[kMultiMaxPairs][kMultiMaxR + 16];  // padded: replacements are read four bytes at a time
+};
+static_assert(sizeof(MultiTable) % 16 == 0, "MultiTable is staged with 16-byte copies");
+
+__host__ __device__ __forceinline__ uint32_t multi_hash(uint32_t b0, uint32_t b1) { return (b0 + 131u * b1) & 255u; }
 
 // Look-back state of tile t: status[t] = (epoch << 2) | state.
 enum TileState : uint32_t { kStAgg = 1, kStInc = 2 };
@@ -97,9 +132,10 @@ struct ReplaceParams {
   unsigned long long len_bias;    // output starts this many bytes into out (out stays 16-byte aligned);
                                   // *len_out receives len_bias + the output length
   unsigned int carry0;
-  unsigned int pad1;
+  unsigned int multi_ratio;       // kModeMulti: output staging per input byte (1..3), as MultiTable::ratio
   const uint8_t* pat_ext;         // device copy when L > kInlineMax
   const uint8_t* rep_ext;         // device copy when R > kInlineMax
+  const MultiTable* multi;        // kModeMulti: the stage's pairs (device memory); L = their longest
   uint8_t pat[kInlineMax];
   uint8_t rep[kInlineMax];
 };
@@ -184,6 +220,18 @@ uint32_t seg_smem_bytes(const SegLaunch& sl);
 int seg_ctas_per_sm(const SegLaunch& sl);
 // Fills a SegPair from (pat, L, rep, R); false when the pair does not fit a segmented launch.
 bool make_seg_pair(SegPair& q, const uint8_t* pat, uint32_t L, const uint8_t* rep, uint32_t R);
+// Partition of a chain of pairs into stages that each run as one pass (kModeMulti when a stage
+// has two pairs or more, the pair's own mode otherwise). stage_of[k] receives the stage of pair
+// k; returns the number of stages. keep_last_alone: the last pair gets a stage of its own.
+int plan_stages(const uint8_t* const* pats, const int* pat_lens, const uint8_t* const* reps,
+                const int* rep_lens, int count, bool keep_last_alone, int* stage_of);
+// Fills a MultiTable from pairs [0, count) (count in [2, kMultiMaxPairs], as plan_stages formed).
+void build_multi_table(MultiTable& T, const uint8_t* const* pats, const int* pat_lens,
+                       const uint8_t* const* reps, const int* rep_lens, int count);
+// Worst-case output length of one pass of a stage over n input bytes (saturating).
+unsigned long long multi_output_bound(const MultiTable& T, unsigned long long n);
+// Launch one stage (p.mode == kModeMulti, p.multi set, p.nsub > 0).
+cudaError_t launch_replace_multi(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out);
 // bytes.replace with an empty pattern: rep before every byte and at the end.
 cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const uint8_t* rep_dev,
                                  uint32_t R, uint8_t* out, cudaStream_t st);

@@ -186,6 +186,23 @@ int cuda_replace_stream(const uint8_t* src, size_t n, const uint8_t** pats, cons
                         const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
                         uint8_t** out_host, size_t* out_len);
 
+/* How cuda_replace_apply_batch groups a chain of pairs into passes (no counterpart in the
+ * reference, whose apply_batch makes one full pass per pair, cuda_replace.cu:2480-2519). A run of
+ * consecutive pairs is one pass (a "stage") when applying them one after the other provably gives
+ * the same bytes as replacing, in the run's input, every occurrence of every pattern of the run at
+ * once: every pattern has no proper border, no two patterns of the run can overlap (none inside
+ * another, no suffix of one equal to a prefix of another, no pattern twice), no replacement of an
+ * earlier pair of the run can form an occurrence of a later pattern with the bytes around it (an
+ * empty replacement joins two bytes, so it ends the run unless the later patterns are one byte
+ * long), and the run has at most 32 pairs, patterns of 1-32 bytes with at most 4 distinct first
+ * bytes, replacements of at most 64 bytes. stage_of[k] receives the pass of pair k; returns the
+ * number of passes, or -1 for invalid arguments. keep_last_alone: the last pair gets a pass of its
+ * own (apply_batch does this, so query_prefix afterwards describes the last pair). Host code only:
+ * needs no GPU. The environment variable CUDA_REPLACE_STAGES=0 makes apply_batch use one pass
+ * per pair. */
+int cuda_replace_plan_stages(const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+                             const int* rep_lens, int count, int keep_last_alone, int* stage_of);
+
 /* Host memcpy on up to 8 threads (large copies): moves a result out of the page-locked
  * block the library returned into memory the caller allocated (in Python: a bytes object
  * created uninitialised), whose first-touch page faults bound a single-threaded copy. No
