@@ -141,7 +141,12 @@ struct Job {
   bool via_session = false;
   int retries = 0;           // segmented reruns after an overflow
   double t_submit = 0, t_done = 0;
+  unsigned int tenant = 0;   // admission is counted against this tenant's budget (0: no budget)
+  size_t charged = 0;        // arena bytes counted against the tenant while the job is placed
 };
+
+constexpr int kCancelled = -8;       // the request was cancelled before it reached the device
+constexpr int kOverTenantBudget = -9;  // the request alone needs more than its tenant's budget
 
 // Largest intermediate length of a job's chain in the worst case (every pattern position a
 // match), capped at `lim`.
@@ -715,10 +720,11 @@ class Server {
   }
 
   int submit(const uint8_t* src, size_t n, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
-             const int* rep_lens, int count, unsigned long long* ticket) {
+             const int* rep_lens, int count, unsigned long long* ticket, unsigned int tenant = 0) {
     auto j = std::make_unique<Job>();
     j->t_submit = now_us();
     j->n = n;
+    j->tenant = tenant;
     j->seg_ok = count <= kMaxRounds;
     for (int i = 0; i < count; ++i) {
       if (pat_lens[i] < 0 || rep_lens[i] < 0 || (pat_lens[i] && !pats[i]) || (rep_lens[i] && !reps[i])) return -1;
@@ -738,6 +744,13 @@ class Server {
     if (n) crb::parallel_memcpy(j->hin, src, n);
     if (j->seg_ok) j->cap = job_capacity(*j);
     std::lock_guard<std::mutex> g(mu_);
+    if (j->seg_ok && tenant) {
+      const auto b = tenant_budget_.find(tenant);
+      if (b != tenant_budget_.end() && Engine::footprint(*j) > b->second) {
+        crb::host_free(j->hin);  // it could never be admitted within the tenant's budget
+        return kOverTenantBudget;
+      }
+    }
     j->ticket = ++next_ticket_;
     *ticket = j->ticket;
     Job* raw = j.get();
@@ -770,6 +783,53 @@ class Server {
     return rc;
   }
 
+  // 0: the request was still queued and is cancelled (a wait then returns kCancelled); 1: it is
+  // on the device, running or done, and completes normally; -1: unknown ticket.
+  int cancel(unsigned long long ticket) {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = jobs_.find(ticket);
+    if (it == jobs_.end()) return -1;
+    Job* j = it->second.get();
+    if (j->done) return 1;
+    auto pi = std::find(pending_.begin(), pending_.end(), j);
+    if (pi != pending_.end()) {
+      pending_.erase(pi);
+    } else {
+      auto fi = std::find(fallback_q_.begin(), fallback_q_.end(), j);
+      if (fi == fallback_q_.end()) return 1;
+      fallback_q_.erase(fi);
+    }
+    crb::host_free(j->hin);
+    j->hin = nullptr;
+    if (j->hout) {
+      crb::host_free(j->hout);
+      j->hout = nullptr;
+    }
+    j->out_len = 0;
+    j->rc = kCancelled;
+    j->done = true;
+    ++cancelled_;
+    cv_.notify_all();
+    return 0;
+  }
+
+  // Device bytes (arena) the tenant's requests may hold at once; 0 removes the limit.
+  void set_tenant_budget(unsigned int tenant, size_t bytes) {
+    std::lock_guard<std::mutex> g(mu_);
+    if (bytes)
+      tenant_budget_[tenant] = bytes;
+    else
+      tenant_budget_.erase(tenant);
+    cv_.notify_all();
+  }
+  void tenant_usage(unsigned int tenant, unsigned long long* in_use, unsigned long long* peak) {
+    std::lock_guard<std::mutex> g(mu_);
+    auto u = tenant_inuse_.find(tenant);
+    auto k = tenant_peak_.find(tenant);
+    *in_use = u == tenant_inuse_.end() ? 0 : u->second;
+    *peak = k == tenant_peak_.end() ? 0 : k->second;
+  }
+
   void stats(CudaReplaceServerStats* st) {
     std::lock_guard<std::mutex> g(mu_);
     memset(st, 0, sizeof(*st));
@@ -781,6 +841,7 @@ class Server {
     st->kernel_launches = eng_.seg_launches;
     st->graph_launches = eng_.graph_launches;
     st->pending = (unsigned long long)(pending_.size() + fallback_q_.size());
+    st->cancelled = cancelled_;
     st->arena_bytes = eng_.arena.size();
     st->arena_peak_bytes = arena_peak_;
     st->gpu_us = (double)eng_.gpu_us.load();
@@ -825,6 +886,14 @@ class Server {
     cv_.notify_all();
   }
 
+  void uncharge(Job* j) {  // with mu_ held
+    if (j->tenant && j->charged) {
+      unsigned long long& u = tenant_inuse_[j->tenant];
+      u = u >= j->charged ? u - j->charged : 0;
+    }
+    j->charged = 0;
+  }
+
   int free_slot() const {
     for (int i = 0; i < kSlots; ++i)
       if (!eng_.slots[i].busy) return i;
@@ -846,22 +915,46 @@ class Server {
       const int si = free_slot();
       Slot& s = eng_.slots[si];
       std::vector<Job*> batch;
-      // admit in arrival order while the job table and the arena (the HBM budget) have room
-      while (!pending_.empty() && (int)batch.size() < eng_.max_jobs) {
-        Job* j = pending_.front();
-        if (!eng_.place(*j)) break;
+      // admit in arrival order while the job table and the arena (the HBM budget) have room; a
+      // request whose tenant has its budget in use waits without holding back other tenants
+      Job* blocked_front = nullptr;  // the oldest request not held back by its tenant
+      for (auto it = pending_.begin(); it != pending_.end() && (int)batch.size() < eng_.max_jobs;) {
+        Job* j = *it;
+        const auto b = j->tenant ? tenant_budget_.find(j->tenant) : tenant_budget_.end();
+        const size_t fp = Engine::footprint(*j);
+        if (b != tenant_budget_.end() && tenant_inuse_[j->tenant] + fp > b->second) {
+          ++it;
+          continue;
+        }
+        if (!eng_.place(*j)) {
+          blocked_front = j;
+          break;
+        }
+        j->charged = fp;
+        if (j->tenant) {
+          const unsigned long long u = (tenant_inuse_[j->tenant] += fp);
+          unsigned long long& pk = tenant_peak_[j->tenant];
+          pk = std::max(pk, u);
+        }
         batch.push_back(j);
-        pending_.pop_front();
+        it = pending_.erase(it);
       }
       if (batch.empty()) {
         bool in_flight = false;
         for (int i = 0; i < kSlots; ++i) in_flight = in_flight || eng_.slots[i].busy;
         if (in_flight) {
-          // the oldest request does not fit beside the batches in flight: wait for one to end
+          // the oldest request does not fit beside the batches in flight, or every queued
+          // request waits for its tenant's requests in flight: wait for a batch to end
           const unsigned long long c0 = completions_;
           cv_.wait(lk, [&] { return !run_ || completions_ != c0; });
-        } else {
+        } else if (blocked_front) {
           // it does not fit in the empty arena (fragmentation or a large request): Session path
+          pending_.erase(std::find(pending_.begin(), pending_.end(), blocked_front));
+          fallback_q_.push_back(blocked_front);
+          cv_.notify_all();
+        } else {
+          // nothing in flight holds a tenant's budget now (a budget was lowered meanwhile): the
+          // oldest request goes to the Session path rather than wait for nothing
           fallback_q_.push_back(pending_.front());
           pending_.pop_front();
           cv_.notify_all();
@@ -881,6 +974,7 @@ class Server {
         // nothing of the batch is trusted: every job goes to the Session path
         for (Job* j : s.jobs) {
           eng_.unplace(*j);
+          uncharge(j);
           fallback_q_.push_back(j);
         }
         s.jobs.clear();
@@ -909,7 +1003,10 @@ class Server {
       for (Job* j : s.jobs)
         if (std::find(rerun.begin(), rerun.end(), j) == rerun.end()) mark_done(j, e == cudaSuccess ? 0 : (int)e);
       lk.lock();
-      for (Job* j : s.jobs) eng_.unplace(*j);
+      for (Job* j : s.jobs) {
+        eng_.unplace(*j);
+        uncharge(j);
+      }
       // an overflowed job runs again, first in the queue, with buffers grown past the length
       // that overflowed (at most twice); otherwise, and after an error, through a Session
       for (auto it = rerun.rbegin(); it != rerun.rend(); ++it) {
@@ -974,7 +1071,10 @@ class Server {
   std::vector<double> lat_;
   unsigned long long jobs_done_ = 0, jobs_session_ = 0, batches_ = 0, bytes_in_ = 0, bytes_out_ = 0;
   unsigned long long arena_peak_ = 0;
+  unsigned long long cancelled_ = 0;
   double session_us_ = 0;
+  std::unordered_map<unsigned int, size_t> tenant_budget_;
+  std::unordered_map<unsigned int, unsigned long long> tenant_inuse_, tenant_peak_;
 };
 
 size_t default_budget() {
@@ -1011,6 +1111,32 @@ CR_EXPORT int cuda_replace_server_submit(void* srv, const uint8_t* src, size_t n
   return static_cast<Server*>(srv)->submit(src, n, pats, pat_lens, reps, rep_lens, count, ticket);
 }
 
+CR_EXPORT int cuda_replace_server_submit_tenant(void* srv, unsigned int tenant, const uint8_t* src, size_t n,
+                                                const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+                                                const int* rep_lens, int count, unsigned long long* ticket) {
+  if (!srv || !ticket || (n && !src) || count < 0 || (count > 0 && (!pats || !pat_lens || !reps || !rep_lens)))
+    return -1;
+  return static_cast<Server*>(srv)->submit(src, n, pats, pat_lens, reps, rep_lens, count, ticket, tenant);
+}
+
+CR_EXPORT int cuda_replace_server_cancel(void* srv, unsigned long long ticket) {
+  if (!srv) return -1;
+  return static_cast<Server*>(srv)->cancel(ticket);
+}
+
+CR_EXPORT int cuda_replace_server_set_tenant_budget(void* srv, unsigned int tenant, size_t bytes) {
+  if (!srv || tenant == 0) return -1;
+  static_cast<Server*>(srv)->set_tenant_budget(tenant, bytes);
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_server_tenant_usage(void* srv, unsigned int tenant, unsigned long long* in_use,
+                                               unsigned long long* peak) {
+  if (!srv || !in_use || !peak) return -1;
+  static_cast<Server*>(srv)->tenant_usage(tenant, in_use, peak);
+  return 0;
+}
+
 CR_EXPORT int cuda_replace_server_wait(void* srv, unsigned long long ticket, int timeout_ms, uint8_t** out_host,
                                        size_t* out_len) {
   if (!srv || !out_host || !out_len) return -1;
@@ -1038,27 +1164,56 @@ CR_EXPORT void cuda_replace_server_close(void* srv) {
   delete s;
 }
 
+namespace {
+// One server per device shared by every cuda_replace_jobs call, opened at the first call and
+// reopened larger when a call's inputs need more device memory; calls are serialised. Released
+// by cuda_replace_jobs_release (the process exit reclaims it otherwise).
+constexpr int kJobsDevices = 64;
+std::mutex g_jobs_mu;
+void* g_jobs_srv[kJobsDevices] = {};
+size_t g_jobs_budget[kJobsDevices] = {};
+}  // namespace
+
 CR_EXPORT int cuda_replace_jobs(int njobs, const uint8_t** srcs, const size_t* src_lens, const int* pair_counts,
                                 const uint8_t** pats, const int* pat_lens, const uint8_t** reps, const int* rep_lens,
                                 uint8_t** out_hosts, size_t* out_lens) {
   if (njobs < 0 || (njobs > 0 && (!srcs || !src_lens || !pair_counts || !out_hosts || !out_lens))) return -1;
   if (njobs == 0) return 0;
-  size_t total_pairs = 0, total_bytes = 0;
+  size_t total_pairs = 0, total_bytes = 0, largest = 0;
   for (int i = 0; i < njobs; ++i) {
     if (pair_counts[i] < 0) return -1;
     total_pairs += (size_t)pair_counts[i];
     total_bytes += src_lens[i];
+    largest = std::max(largest, src_lens[i]);
     out_hosts[i] = nullptr;
     out_lens[i] = 0;
   }
   if (total_pairs && (!pats || !pat_lens || !reps || !rep_lens)) return -1;
-  // a server sized for this call: the inputs with their buffers, within 40% of free memory
-  const size_t budget = std::min(default_budget(), std::max<size_t>(64u << 20, 10 * total_bytes + (64u << 20)));
-  void* srv = nullptr;
-  int rc = cuda_replace_server_open(&srv, budget, std::min(njobs, 4096));
-  if (rc != 0) return rc;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= kJobsDevices) return (int)cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(g_jobs_mu);
+  // device memory for this call: its inputs with their ping-pong buffers (about 9 bytes per input
+  // byte), at least room for its largest job, within 40% of the free memory
+  const size_t want = std::max<size_t>(64u << 20, std::min<size_t>(9 * total_bytes, 9 * largest + (512u << 20)));
+  if (!g_jobs_srv[dev] || g_jobs_budget[dev] < std::min(want, default_budget() + g_jobs_budget[dev])) {
+    if (g_jobs_srv[dev]) {
+      cuda_replace_server_close(g_jobs_srv[dev]);
+      g_jobs_srv[dev] = nullptr;
+    }
+    const size_t budget = std::min(default_budget(), std::max(want, (size_t)256 << 20));
+    int rc = cuda_replace_server_open(&g_jobs_srv[dev], budget, 4096);
+    if (rc != 0) {
+      g_jobs_srv[dev] = nullptr;
+      return rc;
+    }
+    g_jobs_budget[dev] = budget;
+  }
+  void* srv = g_jobs_srv[dev];
   std::vector<unsigned long long> tickets((size_t)njobs, 0);
   size_t p = 0;
+  int rc = 0;
   for (int i = 0; i < njobs && rc == 0; ++i) {
     rc = cuda_replace_server_submit(srv, srcs[i], src_lens[i], pats ? pats + p : nullptr,
                                     pat_lens ? pat_lens + p : nullptr, reps ? reps + p : nullptr,
@@ -1071,7 +1226,6 @@ CR_EXPORT int cuda_replace_jobs(int njobs, const uint8_t** srcs, const size_t* s
     const int r = cuda_replace_server_wait(srv, tickets[(size_t)i], -1, &out_hosts[i], &out_lens[i]);
     if (r != 0 && first_err == 0) first_err = r;
   }
-  cuda_replace_server_close(srv);
   if (first_err != 0)
     for (int i = 0; i < njobs; ++i)
       if (out_hosts[i]) {
@@ -1080,4 +1234,18 @@ CR_EXPORT int cuda_replace_jobs(int njobs, const uint8_t** srcs, const size_t* s
         out_lens[i] = 0;
       }
   return first_err;
+}
+
+CR_EXPORT void cuda_replace_jobs_release(void) {
+  std::lock_guard<std::mutex> g(g_jobs_mu);
+  for (int d = 0; d < kJobsDevices; ++d)
+    if (g_jobs_srv[d]) {
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(d);
+      cuda_replace_server_close(g_jobs_srv[d]);
+      cudaSetDevice(cur);
+      g_jobs_srv[d] = nullptr;
+      g_jobs_budget[d] = 0;
+    }
 }

@@ -87,7 +87,8 @@ class ServerStats(C.Structure):
                 ("graph_launches", C.c_ulonglong), ("pending", C.c_ulonglong), ("arena_bytes", C.c_ulonglong),
                 ("arena_peak_bytes", C.c_ulonglong), ("p50_us", C.c_double), ("p99_us", C.c_double),
                 ("max_us", C.c_double), ("gpu_us", C.c_double), ("download_us", C.c_double),
-                ("session_us", C.c_double), ("tile_bytes", C.c_uint * 3), ("grid_ctas", C.c_int * 3)]
+                ("session_us", C.c_double), ("tile_bytes", C.c_uint * 3), ("grid_ctas", C.c_int * 3),
+                ("cancelled", C.c_ulonglong)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -140,6 +141,13 @@ class CudaReplaceLib:
         _bind(lib, "cuda_replace_server_submit",
               [c_void_p, c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int,
                C.POINTER(C.c_ulonglong)], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_submit_tenant",
+              [c_void_p, C.c_uint, c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int,
+               C.POINTER(C.c_ulonglong)], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_cancel", [c_void_p, C.c_ulonglong], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_set_tenant_budget", [c_void_p, C.c_uint, c_size_t], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_server_tenant_usage",
+              [c_void_p, C.c_uint, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)], C.c_int, optional=True)
         _bind(lib, "cuda_replace_server_wait",
               [c_void_p, C.c_ulonglong, C.c_int, C.POINTER(c_uint8_p), c_size_t_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_server_stats", [c_void_p, C.POINTER(ServerStats)], C.c_int, optional=True)
@@ -148,6 +156,9 @@ class CudaReplaceLib:
         _bind(lib, "cuda_replace_jobs",
               [C.c_int, c_uint8_pp, c_size_t_p, c_int_p, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p,
                c_uint8_pp, c_size_t_p], C.c_int, optional=True)
+        _bind(lib, "cuda_replace_jobs_release", [], None, optional=True)
+        _bind(lib, "cuda_replace_plan_stages",
+              [c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, C.c_int, c_int_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_host_copy", [c_void_p, c_void_p, c_size_t], None, optional=True)
         _bind(lib, "cuda_replace_stream",
               [c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t,
@@ -314,6 +325,10 @@ class Session:
             self.h = c_void_p(None)
 
 
+class CancelledJob(Exception):
+    """Server.wait on a job that Server.cancel removed from the queue."""
+
+
 class Server:
     """Request loop over batched segmented launches (no counterpart in the reference).
 
@@ -338,17 +353,43 @@ class Server:
     def __exit__(self, exc_type, exc, tb):
         self.close()
 
-    def submit(self, data, pairs: Sequence[Tuple[bytes, bytes]]) -> int:
+    def submit(self, data, pairs: Sequence[Tuple[bytes, bytes]], tenant: int = 0) -> int:
+        """Queue a job; tenant >= 1 counts its device memory against that tenant's budget."""
         keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(pairs)
         holder, src_ptr, n = _src_pointer(data)
         ticket = C.c_ulonglong(0)
-        rc = self.lib.lib.cuda_replace_server_submit(
-            self.h, src_ptr, c_size_t(n), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
-            C.cast(rep_ptrs, c_uint8_pp), C.cast(rep_lens, c_int_p), C.c_int(len(pairs)), C.byref(ticket))
+        args = (src_ptr, c_size_t(n), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
+                C.cast(rep_ptrs, c_uint8_pp), C.cast(rep_lens, c_int_p), C.c_int(len(pairs)), C.byref(ticket))
+        if tenant:
+            rc = self.lib.lib.cuda_replace_server_submit_tenant(self.h, C.c_uint(tenant), *args)
+        else:
+            rc = self.lib.lib.cuda_replace_server_submit(self.h, *args)
         del keep, holder
+        if rc == -9:
+            raise MemoryError(f"the job needs more device memory than tenant {tenant}'s budget")
         if rc != 0:
             raise RuntimeError(f"cuda_replace_server_submit failed rc={rc}")
         return int(ticket.value)
+
+    def cancel(self, ticket: int) -> bool:
+        """True when the job was still queued and is cancelled (its wait then raises
+        CancelledJob); False when it is already on the device or done (it completes normally)."""
+        rc = self.lib.lib.cuda_replace_server_cancel(self.h, C.c_ulonglong(ticket))
+        if rc < 0:
+            raise KeyError(ticket)
+        return rc == 0
+
+    def set_tenant_budget(self, tenant: int, nbytes: int) -> None:
+        """Device memory that tenant's jobs may hold at once (0: no limit)."""
+        rc = self.lib.lib.cuda_replace_server_set_tenant_budget(self.h, C.c_uint(tenant), c_size_t(int(nbytes)))
+        if rc != 0:
+            raise RuntimeError(f"cuda_replace_server_set_tenant_budget failed rc={rc}")
+
+    def tenant_usage(self, tenant: int) -> Tuple[int, int]:
+        """(bytes the tenant's jobs hold on the device now, the most they held at once)."""
+        cur, peak = C.c_ulonglong(0), C.c_ulonglong(0)
+        self.lib.lib.cuda_replace_server_tenant_usage(self.h, C.c_uint(tenant), C.byref(cur), C.byref(peak))
+        return int(cur.value), int(peak.value)
 
     def wait(self, ticket: int, timeout_ms: int = -1) -> Optional[bytes]:
         """The job's result; None when it is not done within timeout_ms (negative: no limit)."""
@@ -358,6 +399,8 @@ class Server:
                                                    C.byref(out_ptr), C.byref(out_len))
         if rc == 1:
             return None
+        if rc == -8:
+            raise CancelledJob(ticket)
         if rc != 0:
             raise RuntimeError(f"cuda_replace_server_wait failed rc={rc}")
         try:

@@ -242,6 +242,7 @@ typedef struct CudaReplaceServerStats {
   double session_us;                    /* jobs run through a Session, host wall time */
   unsigned int tile_bytes[3];           /* autotuned super-tile bytes: free, bordered L<=4, bordered L<=32 */
   int grid_ctas[3];
+  unsigned long long cancelled;         /* requests cancelled before they reached the device */
 } CudaReplaceServerStats;
 
 int cuda_replace_server_open(void** srv, size_t hbm_budget, int max_jobs_per_batch);
@@ -251,9 +252,29 @@ int cuda_replace_server_submit(void* srv, const uint8_t* src, size_t n,
                                const uint8_t** pats, const int* pat_lens,
                                const uint8_t** reps, const int* rep_lens, int count,
                                unsigned long long* ticket);
+/* As cuda_replace_server_submit, for a tenant (tenant 0: none). While the tenant's budget (see
+ * cuda_replace_server_set_tenant_budget) is in use by its requests on the device, its further
+ * requests wait in the queue without holding back other tenants' requests. -9: the request alone
+ * needs more device memory than its tenant's budget. */
+int cuda_replace_server_submit_tenant(void* srv, unsigned int tenant, const uint8_t* src, size_t n,
+                                      const uint8_t** pats, const int* pat_lens,
+                                      const uint8_t** reps, const int* rep_lens, int count,
+                                      unsigned long long* ticket);
+/* Cancel a request that is still queued: returns 0 and its wait then returns -8 (cancelled)
+ * with no result; 1 when the request is already on the device, running or done (it completes
+ * normally); -1 for an unknown ticket. */
+int cuda_replace_server_cancel(void* srv, unsigned long long ticket);
+/* Device memory (bytes of the server's arena) that requests of tenant (>= 1) may hold at once;
+ * 0 removes the limit. Requests of a tenant without a budget share the whole arena. Requests
+ * that run through a Session instead of a batch use no arena memory and are not counted. */
+int cuda_replace_server_set_tenant_budget(void* srv, unsigned int tenant, size_t bytes);
+/* Arena bytes held by a tenant's requests now and at most since the server opened. */
+int cuda_replace_server_tenant_usage(void* srv, unsigned int tenant, unsigned long long* in_use,
+                                     unsigned long long* peak);
 /* 0: done; *out_host (page-locked, release with cuda_free_host; NULL when empty) and
  * *out_len receive the result and the ticket is retired. 1: not done within timeout_ms
- * (negative: wait without limit). -1: unknown ticket. Other: the request's error code. */
+ * (negative: wait without limit). -1: unknown ticket. -8: cancelled (retired, no result).
+ * Other: the request's error code. */
 int cuda_replace_server_wait(void* srv, unsigned long long ticket, int timeout_ms,
                              uint8_t** out_host, size_t* out_len);
 int cuda_replace_server_stats(void* srv, CudaReplaceServerStats* stats);
@@ -263,11 +284,16 @@ void cuda_replace_server_close(void* srv);
 
 /* One call for many jobs: job i is srcs[i][0, src_lens[i]) with pair_counts[i] pairs, the
  * pairs of all jobs concatenated in pats/pat_lens/reps/rep_lens. out_hosts[i] / out_lens[i]
- * receive job i's result (release each with cuda_free_host). Runs on a server opened for the
- * call. On an error no result is returned. */
+ * receive job i's result (release each with cuda_free_host). Runs on one server per device that
+ * every call shares: opened by the first call with device memory for its inputs (about nine
+ * bytes per input byte, at least 256 MiB, at most 40% of the free memory) and reopened larger
+ * when a later call needs more; calls are serialised. On an error no result is returned. */
 int cuda_replace_jobs(int njobs, const uint8_t** srcs, const size_t* src_lens, const int* pair_counts,
                       const uint8_t** pats, const int* pat_lens, const uint8_t** reps, const int* rep_lens,
                       uint8_t** out_hosts, size_t* out_lens);
+/* Close the server that cuda_replace_jobs keeps and release its device and page-locked memory
+ * (the next call opens a new one). */
+void cuda_replace_jobs_release(void);
 
 #ifdef __cplusplus
 }

@@ -150,3 +150,55 @@ def test_server_overflow_reruns_segmented(cr_lib):
     assert st["jobs_via_session"] == 0
     for i, ((data, pairs), out) in enumerate(zip(jobs, outs)):
         assert out == chain(data, pairs), i
+
+
+def test_server_cancel_queued_jobs(cr_lib):
+    """Jobs cancelled while still queued give no result (their wait raises CancelledJob); jobs
+    already on the device complete normally; every completed result is exact."""
+    jobs = [WL.c5_job(i, min_size=1 << 20, max_size=4 << 20) for i in range(64)]
+    with Wr.Server(cr_lib, max_jobs_per_batch=2) as srv:
+        tickets = [srv.submit(j.data, j.pairs) for j in jobs]
+        cancelled = {t for t in tickets[16:] if srv.cancel(t)}
+        assert cancelled, "no queued job could be cancelled"
+        for j, t in zip(jobs, tickets):
+            if t in cancelled:
+                with pytest.raises(Wr.CancelledJob):
+                    srv.wait(t)
+            else:
+                assert srv.wait(t) == chain(j.data, j.pairs)
+        assert srv.stats()["cancelled"] == len(cancelled)
+        with pytest.raises(KeyError):
+            srv.cancel(tickets[0])  # retired by its wait
+
+
+def test_server_tenant_budgets(cr_lib):
+    """A tenant's jobs never hold more device memory than its budget at once, they do not hold
+    back another tenant's jobs, and a job larger than its tenant's whole budget is refused."""
+    jobs = [WL.c5_job(i, min_size=256 << 10, max_size=2 << 20) for i in range(48)]
+    with Wr.Server(cr_lib) as srv:
+        budget = 24 << 20
+        srv.set_tenant_budget(1, budget)
+        tickets = [(j, srv.submit(j.data, j.pairs, tenant=1 + (i % 2))) for i, j in enumerate(jobs)]
+        for j, t in tickets:
+            assert srv.wait(t) == chain(j.data, j.pairs)
+        cur, peak = srv.tenant_usage(1)
+        assert cur == 0 and 0 < peak <= budget
+        _, peak2 = srv.tenant_usage(2)
+        assert peak2 > 0  # tenant 2 has no budget: it only shares the arena
+        with pytest.raises(MemoryError):
+            srv.submit(b"a" * (32 << 20), [(b"a", b"b")], tenant=1)
+
+
+def test_replace_jobs_shared_server_reused(cr_lib):
+    """cuda_replace_jobs keeps one server between calls (opened by the first, grown when a call
+    needs more memory) and releases it on request; results stay exact across the calls."""
+    small = small_c5_jobs(40)
+    for _ in range(3):
+        outs = Wr.replace_jobs(cr_lib, small)
+        assert all(o == chain(d, p) for (d, p), o in zip(small, outs))
+    large = [(WL.c5_job(i, min_size=8 << 20, max_size=24 << 20).data, [(b"\x01", b"xy")]) for i in range(6)]
+    outs = Wr.replace_jobs(cr_lib, large)
+    assert all(o == chain(d, p) for (d, p), o in zip(large, outs))
+    cr_lib.lib.cuda_replace_jobs_release()
+    outs = Wr.replace_jobs(cr_lib, small[:5])
+    assert all(o == chain(d, p) for (d, p), o in zip(small[:5], outs))

@@ -186,25 +186,52 @@ def test_c5_jobs_match_reference(refw, libs):
 
 
 # ------------------------------------------------------------------ seeded applies and queries
-@pytest.mark.parametrize("src,pat,rep", [
-    (b"aaaaaaaaaa" * 1000, b"aa", b"X"),
-    (b"abababab" * 3000 + b"ab", b"abab", b"Z"),
-    (b"hello world " * 5000, b"lo", b"LOL"),
-    (b"xxxaayyy" * 4000, b"aa", b""),
-])
-def test_seeded_apply_and_query_prefix_match_reference(refw, libs, src, pat, rep):
-    """apply_seeded with the unseeded sentinel (py:313) and with non-negative seeds, which both
-    libraries honour, then query_prefix at limits across the buffer (the calls streaming
-    makes, py:347-355). out_last_rel is not compared: the reference's fused path leaves it
-    stale (cu:929-934)."""
-    for seed in (-(1 << 29), 0, 1, 5, 101):
+SEEDED = [
+    ("a-run aa->X", b"a" * 8000, b"aa", b"X"),
+    ("abab->Z", b"abababab" * 750 + b"ab", b"abab", b"Z"),
+    ("lo->LOL", b"hello world " * 600, b"lo", b"LOL"),
+    ("aa->''", b"xxxaayyy" * 1000, b"aa", b""),
+]
+SEEDS = (-(1 << 29), 0, 1, 5, 101)
+
+
+@pytest.mark.parametrize("name,src,pat,rep", SEEDED, ids=[c[0] for c in SEEDED])
+def test_seeded_apply_and_query_prefix_match_reference(refw, libs, oracle_mod, name, src, pat, rep):
+    """apply_seeded with the unseeded sentinel (py:313) and with non-negative seeds, then
+    query_prefix at limits across the buffer (the calls streaming makes, py:347-355): the new
+    library equals the C oracle, and the reference equals the new library. Inputs stay within
+    one of the reference's 8 KiB fused tiles (FUSED_TILE_BYTES, cu:79), where its seeded greedy
+    is exact; out_last_rel is not compared (the reference's fused path leaves it stale,
+    cu:929-934)."""
+    limits = (0, 1, 2, 3, 17, 4095, 4096, 4097, len(src) // 2, len(src))
+    for seed in SEEDS:
+        bb = oracle_mod.block_before_from_seed(None if seed <= -(1 << 28) else seed, len(pat))
+        want_out, _, _ = oracle_mod.replace(src, pat, rep, bb)
+        want_q = [oracle_mod.query_prefix(src, pat, lim, bb) for lim in limits]
         answers = []
         for lib in libs:
             with refw.Session(lib, src) as s:
                 new_len, _ = s.apply_seeded(pat, rep, seed)
-                qs = [s.query_prefix(lim) for lim in (0, 1, 2, 3, 17, 8191, 8192, 8193, len(src) // 2, len(src))]
+                qs = [s.query_prefix(lim) for lim in limits]
                 answers.append((new_len, qs, s.result()))
-        assert answers[0] == answers[1], f"seed {seed}"
+        assert answers[0] == (len(want_out), want_q, want_out), f"seed {seed}"
+        assert answers[1] == answers[0], f"seed {seed}"
+
+
+def test_d1_seeded_tile_carry_reference_differs(refw, libs, oracle_mod):
+    """A seeded apply over a self-overlapping run longer than the reference's 8 KiB fused tile:
+    an odd seed shifts the greedy's parity in tile 0, but the reference seeds tile 1 from
+    tile 0's unseeded pass (cu:737-884), so its output differs (D1). The new library equals
+    the oracle."""
+    src, pat, rep, seed = b"a" * 10000, b"aa", b"X", 1
+    want, _, _ = oracle_mod.replace(src, pat, rep, oracle_mod.block_before_from_seed(seed, 2))
+    outs = []
+    for lib in libs:
+        with refw.Session(lib, src) as s:
+            s.apply_seeded(pat, rep, seed)
+            outs.append(s.result())
+    assert outs[0] == want
+    assert outs[1] != want
 
 
 # ------------------------------------------------------------------ streaming helper
