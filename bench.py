@@ -348,7 +348,8 @@ def run_ours(args, dist: Dist):
                  "e2e_pageable": pageable_e2e(lib, n_run, rand_np),
                  "chain_128_pairs": chain_figures(lib, 4 * GiB if args.scale >= 1.0 else int(256 * MiB * args.scale) + MiB,
                                                   2, 1),
-                 "stream_8_pairs": stream_figures(lib, 16 * GiB if args.scale >= 1.0 else int(GiB * args.scale) + MiB, 1)}
+                 "stream_8_pairs": stream_figures(lib, 16 * GiB if args.scale >= 1.0 else int(GiB * args.scale) + MiB, 1),
+                 "sparse_index": index_figures(lib, GiB if args.scale >= 1.0 else int(256 * MiB * args.scale) + MiB)}
 
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
@@ -624,6 +625,45 @@ def stream_figures(lib, total: int, steps: int) -> dict:
             "h2d_bytes": total, "d2h_bytes": len(out), "host_link_gbs": round((total + len(out)) / t / 1e9, 3),
             "api": "gpu_replace_streaming (Python bytes in, Python bytes out)", "steps": len(times),
             "check": digest}
+
+
+def index_figures(lib, total: int) -> dict:
+    """A sparse pattern (64 planted NEEDLE tokens in tiled Zipf text, whose first byte occurs
+    nowhere else) with and without the presence index (cuda_replace_build_index): apply time
+    (host clock around the synchronous call, input resident), and the index build time."""
+    from cuda_replace_b200 import workloads as WL
+    from cuda_replace_b200.cuda_replace_wrapper import Session
+    import random
+    txt = bytearray(WL.tiled_text(total, seed=3))
+    rng = random.Random(9)
+    for _ in range(64):
+        pos = rng.randrange(len(txt) - 8)
+        txt[pos:pos + 6] = b"NEEDLE"
+    txt = bytes(txt)
+    want_len = len(txt) - 64 * 1 if txt.count(b"NEEDLE") == 64 else None
+    res = {}
+    with Session(lib, txt) as s:
+        for arm in ("scan", "index"):
+            t_apply, t_build = [], []
+            for it in range(4):
+                s.reset(txt)
+                t0 = time.perf_counter()
+                if arm == "index":
+                    s.build_index()
+                t1 = time.perf_counter()
+                n = s.apply(b"NEEDLE", b"FOUND")
+                t2 = time.perf_counter()
+                if want_len is not None and n != want_len:
+                    raise SystemExit(f"index self-check failed ({arm}): {n} != {want_len}")
+                if it:
+                    t_apply.append(t2 - t1)
+                    t_build.append(t1 - t0)
+            res[arm] = (statistics.median(t_apply), statistics.median(t_build))
+    (ta, _), (ti, tb) = res["scan"], res["index"]
+    return {"workload": f"{total / GiB:g} GiB tiled Zipf text, 64 x NEEDLE -> FOUND", "apply_ms": round(ta * 1e3, 3),
+            "apply_ms_with_index": round(ti * 1e3, 3), "build_index_ms": round(tb * 1e3, 3),
+            "gbs_in_out": round(2 * total / ta / 1e9, 1), "gbs_in_out_with_index": round(2 * total / ti / 1e9, 1),
+            "timer": "host clock around the synchronous call (includes its 96-byte read-back)"}
 
 
 def c1_figures(lib, dev) -> dict:

@@ -143,6 +143,11 @@ struct Session {
   unsigned long long* lens = nullptr;       // device: lengths along an apply_batch chain
   unsigned long long* lens_host = nullptr;  // page-locked mirror
   size_t lens_cap = 0;
+  unsigned long long buf_version = 1;       // changes whenever the contents of buf change
+  uint32_t* pres = nullptr;                 // presence index of buf (cuda_replace_build_index)
+  size_t pres_cap = 0;                      // words
+  uint32_t pres_shift = 20;
+  unsigned long long pres_version = 0;      // buf_version the index describes (0: none)
   crb::MultiTable* mtab = nullptr;          // device: pair tables of an apply_batch's stages
   crb::MultiTable* mtab_host = nullptr;     // page-locked mirror
   size_t mtab_cap = 0;
@@ -278,6 +283,7 @@ void session_free(Session* s) {
   if (s->ext_host) cudaFreeHost(s->ext_host);
   if (s->lens) cudaFree(s->lens);
   if (s->lens_host) cudaFreeHost(s->lens_host);
+  if (s->pres) cudaFree(s->pres);
   if (s->mtab) cudaFree(s->mtab);
   if (s->mtab_host) cudaFreeHost(s->mtab_host);
   for (int k = 0; k < kUnifiedChunks; ++k) {
@@ -368,6 +374,7 @@ int session_load(Session* s, const uint8_t* src, size_t len) {
   e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return (int)e;
   s->len = len;
+  ++s->buf_version;
   s->q_kind = 0;
   return 0;
 }
@@ -450,6 +457,7 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
     e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) return (int)e;
     swap_buffers(s);
+    ++s->buf_version;
     s->len = out_n;
     s->q_kind = 3;
     s->q_n = n;
@@ -500,6 +508,10 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
   p.in = s->buf;
   p.n = n;
   p.block_before = block_before;
+  if (s->pres_version == s->buf_version && p.nsub) {  // the presence index describes this input
+    p.presence = s->pres;
+    p.presence_shift = s->pres_shift;
+  }
   p.status = s->status;
   p.incl = s->incl;
   p.agg = s->agg;
@@ -525,6 +537,7 @@ int apply_one(Session* s, const uint8_t* pat, int pat_len, const uint8_t* rep, i
       continue;
     }
     swap_buffers(s);
+    ++s->buf_version;
     s->len = (size_t)r.out_len;
     s->q_kind = 2;
     s->q_n = n;
@@ -622,7 +635,8 @@ int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, c
     s->lens_cap = cap;
   }
   if (tabs.size() > s->mtab_cap) {
-    if (s->mtab) cudaFree(s->mtab);
+    if (s->pres) cudaFree(s->pres);
+  if (s->mtab) cudaFree(s->mtab);
     if (s->mtab_host) cudaFreeHost(s->mtab_host);
     s->mtab = nullptr;
     s->mtab_host = nullptr;
@@ -662,7 +676,13 @@ int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, c
     p.tile_last = s->tile_last;
     p.rec = s->rec;
     p.epoch = next_epoch(s);
-    if (k == 0) first_epoch = p.epoch;
+    if (k == 0) {
+      first_epoch = p.epoch;
+      if (s->pres_version == s->buf_version) {  // the presence index describes the first input
+        p.presence = s->pres;
+        p.presence_shift = s->pres_shift;
+      }
+    }
     if (tab_of[(size_t)k] >= 0) {
       p.multi = s->mtab + tab_of[(size_t)k];
       e = crb::launch_replace_multi(p, s->stream, nullptr);
@@ -684,6 +704,7 @@ int apply_batch_chained(Session* s, const uint8_t** pats, const int* pat_lens, c
       (r.overflow_epoch >= first_epoch && r.overflow_epoch <= last_epoch))
     return kErrUnknown;
   if (nst & 1) swap_buffers(s);
+  ++s->buf_version;
   s->len = (size_t)s->lens_host[nst];
   ReplaceParams q = ps[(size_t)nst - 1];  // a single pair (the last pair runs alone)
   q.n = s->lens_host[nst - 1];
@@ -847,8 +868,31 @@ CR_EXPORT int cuda_replace_reset(void* h, const uint8_t* src, size_t len) {
 }
 
 CR_EXPORT int cuda_replace_build_index(void* h, size_t chunk_size) {
-  (void)chunk_size;
   SESSION_GUARD(h);
+  // chunk: the reference's default of 1 MiB (DEFAULT_CHUNK_SIZE, cu:70), else the next power of
+  // two of at least 16 KiB (a sub-tile of the kernel must lie inside one chunk)
+  uint32_t shift = 20;
+  if (chunk_size) {
+    shift = 14;
+    while (shift < 40 && ((size_t)1 << shift) < chunk_size) ++shift;
+  }
+  s->pres_version = 0;
+  if (s->len == 0) return 0;
+  const size_t chunks = (s->len + ((size_t)1 << shift) - 1) >> shift;
+  if (chunks * 8 > s->pres_cap) {
+    if (s->pres) cudaFree(s->pres);
+    s->pres = nullptr;
+    s->pres_cap = 0;
+    cudaError_t e = cudaMalloc(&s->pres, chunks * 8 * sizeof(uint32_t));
+    if (e != cudaSuccess) return (int)e;
+    s->pres_cap = chunks * 8;
+  }
+  cudaError_t e = crb::launch_presence(s->buf, s->len, shift, s->pres, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return (int)e;
+  ++s->launches;
+  s->pres_shift = shift;
+  s->pres_version = s->buf_version;
   return 0;
 }
 
@@ -1159,6 +1203,7 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   if (rc == 0 && e1 != cudaSuccess) rc = (int)e1;
   if (rc == 0 && e2 != cudaSuccess) rc = (int)e2;
   s->len = 0;  // the session's buffers hold no complete content now
+  ++s->buf_version;
   s->q_kind = 0;
   if (rc != 0 || O == 0) {
     pinned_pool().put(host);

@@ -136,6 +136,12 @@ struct ReplaceParams {
   const uint8_t* pat_ext;         // device copy when L > kInlineMax
   const uint8_t* rep_ext;         // device copy when R > kInlineMax
   const MultiTable* multi;        // kModeMulti: the stage's pairs (device memory); L = their longest
+  // Presence index of the input (cuda_replace_build_index): 8 words (a 256-bit byte set) per
+  // chunk of 2^presence_shift bytes (>= 16 KiB). A 16 KiB sub-tile whose chunk lacks the
+  // pattern's first byte has no candidate and skips the search. nullptr: no index.
+  const uint32_t* presence;
+  unsigned int presence_shift;
+  unsigned int pad2;
   uint8_t pat[kInlineMax];
   uint8_t rep[kInlineMax];
 };
@@ -232,6 +238,10 @@ void build_multi_table(MultiTable& T, const uint8_t* const* pats, const int* pat
 unsigned long long multi_output_bound(const MultiTable& T, unsigned long long n);
 // Launch one stage (p.mode == kModeMulti, p.multi set, p.nsub > 0).
 cudaError_t launch_replace_multi(const ReplaceParams& p, cudaStream_t st, int* grid_ctas_out);
+// Presence index: for every chunk of 2^shift bytes of in[0, n), the set of byte values in it
+// (8 words, bit b of word b / 32) into masks[8 * chunk ...].
+cudaError_t launch_presence(const uint8_t* in, unsigned long long n, uint32_t shift, uint32_t* masks,
+                            cudaStream_t st);
 // bytes.replace with an empty pattern: rep before every byte and at the end.
 cudaError_t launch_empty_pattern(const uint8_t* in, unsigned long long n, const uint8_t* rep_dev,
                                  uint32_t R, uint8_t* out, cudaStream_t st);

@@ -69,8 +69,12 @@ int cuda_replace_open(void** ph, const uint8_t* src, size_t len);
  * Replaces cuda_replace_reset (cuda_replace.cu:2295); bound at cuda_replace_wrapper.py:97-101. */
 int cuda_replace_reset(void* h, const uint8_t* src, size_t len);
 
-/* Accepted for compatibility and does nothing: the reference builds a presence index
- * here that no apply path consults (cuda_replace.cu:1249, 1904, 2006).
+/* Build a presence index of the session buffer: for every chunk of chunk_size bytes (0: 1 MiB,
+ * the reference's default; otherwise rounded up to a power of two of at least 16 KiB) the set of
+ * byte values it holds. The next apply, apply_seeded or apply_batch (its first pair) of this
+ * buffer skips the candidate search in every 16 KiB sub-tile whose chunk lacks the pattern's
+ * first byte; results are unchanged. Any change of the buffer (reset, apply) retires the index.
+ * The reference builds the same kind of index but no apply path consults it (cu:1249, 1904, 2006).
  * Replaces cuda_replace_build_index (cuda_replace.cu:2320); bound at cuda_replace_wrapper.py:65-69. */
 int cuda_replace_build_index(void* h, size_t chunk_size);
 
