@@ -21,7 +21,10 @@
 // next chunk's upload overlaps this chunk's stages and the previous chunk's download.
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
 #include <cstdint>
 #include <cstring>
 #include <thread>
@@ -41,6 +44,7 @@ using crb::TileIncl;
 
 constexpr int kErrUnknown = 999;  // cudaErrorUnknown
 constexpr int kUnsupported = -7;  // a pair outside the limits of this path
+constexpr int kIoError = -10;     // reading the input or writing the output file failed (errno is kept)
 
 size_t rup(size_t x, size_t q) { return (x + q - 1) / q * q; }
 
@@ -284,10 +288,11 @@ struct Stream {
   }
 };
 
-int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
-                   const int* rep_lens, int count, size_t chunk_bytes, uint8_t** out_host, size_t* out_len) {
+// Pair checks, buffers, streams and initial carries of a chunk-major stream over chunks of
+// `chunk` bytes. staging: page-locked buffers for the chunks (S.hin) are needed.
+int stream_setup(Stream& S, const uint8_t** pats, const int* pat_lens, const uint8_t** reps, const int* rep_lens,
+                 int count, size_t chunk, bool staging) {
   crb::PinnedPool& pool = crb::host_pinned_pool();
-  Stream S;
   S.count = count;
   S.st.resize((size_t)count);
   for (int k = 0; k < count; ++k) {
@@ -304,9 +309,7 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
     if (rl) memcpy(p.rep, reps[k], (size_t)rl);
     S.st[(size_t)k].P = (uint32_t)pl - 1;
   }
-  if (n == 0) return 0;  // every pair has a pattern: nothing matches in an empty input
-  S.chunk = std::max<size_t>(1, std::min(chunk_bytes ? chunk_bytes : (256u << 20), n));
-  const bool src_pinned = is_pinned(src);
+  S.chunk = chunk;
   cudaError_t e = cudaStreamCreateWithFlags(&S.comp, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S.h2d, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S.d2h, cudaStreamNonBlocking);
@@ -318,7 +321,7 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
   S.in0_cap = S.st[0].P + S.chunk;
   for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
     e = cudaMalloc(&S.in0[b], rup(S.in0_cap, 1u << 20) + 64);
-    if (e == cudaSuccess && !src_pinned) S.hin[b] = static_cast<uint8_t*>(pool.get(S.chunk, &e));
+    if (e == cudaSuccess && staging) S.hin[b] = static_cast<uint8_t*>(pool.get(S.chunk, &e));
   }
   for (int k = 0; k < count && e == cudaSuccess; ++k)
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
@@ -335,14 +338,75 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
   if (e == cudaSuccess) e = cudaMallocHost(&S.meta_host, (size_t)(count + 2) * sizeof(unsigned long long));
   if (e == cudaSuccess) e = S.size_buffers();
   if (e != cudaSuccess) return (int)e;
-  {
-    // every stage starts with its P held bytes covered: at the first chunk they do not exist
-    std::vector<unsigned int> c0((size_t)2 * count, 0u);
-    for (int k = 0; k < count; ++k) c0[(size_t)2 * k] = S.st[(size_t)k].P;
-    e = cudaMemcpyAsync(S.carry, c0.data(), c0.size() * sizeof(unsigned int), cudaMemcpyHostToDevice, S.comp);
+  // every stage starts with its P held bytes covered: at the first chunk they do not exist
+  std::vector<unsigned int> c0((size_t)2 * count, 0u);
+  for (int k = 0; k < count; ++k) c0[(size_t)2 * k] = S.st[(size_t)k].P;
+  e = cudaMemcpyAsync(S.carry, c0.data(), c0.size() * sizeof(unsigned int), cudaMemcpyHostToDevice, S.comp);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(S.comp);
+  return (int)e;
+}
+
+// Enqueue every stage of chunk c (in parity b, m new bytes), wait for it, and grow the buffer
+// that overflowed and run it again until it fits. after_enqueue runs once, on the host, while
+// the first attempt computes (the next chunk's upload, file I/O). Returns 0 or an error code.
+template <typename F>
+int run_chunk_fitting(Stream& S, int b, size_t m, bool first, bool final, F&& after_enqueue) {
+  for (int attempt = 0;; ++attempt) {
+    cudaError_t e = cudaStreamWaitEvent(S.comp, S.ev_h2d[b], 0);
+    uint32_t e0 = 0;
+    if (e == cudaSuccess) e = S.run_chunk(b, m, first, final, &e0);
+    if (e == cudaSuccess && attempt == 0) e = after_enqueue();  // overlaps this chunk's stages
     if (e == cudaSuccess) e = cudaStreamSynchronize(S.comp);
     if (e != cudaSuccess) return (int)e;
+    const ApplyResult r = *S.res_host;
+    const uint32_t e1 = e0 + (uint32_t)S.count - 1u;
+    if (r.error_epoch >= e0 && r.error_epoch <= e1) return kErrUnknown;  // a bounded wait gave up
+    if (!(r.overflow_epoch >= e0 && r.overflow_epoch <= e1)) return 0;
+    // The chunk's inputs (in0[b], pend[b], the carries of parity b) are intact: grow the buffer
+    // that overflowed and run the chunk again. The first stage whose output length passed its
+    // buffer is the one that overflowed (later stages read a clamped input); that length is
+    // exact, so one regrow per stage suffices.
+    int k = S.count - 1;
+    unsigned long long need = S.meta_host[S.count];
+    for (int j = 0; j + 1 < S.count; ++j)
+      if (S.meta_host[j + 1] > S.xcap) {
+        k = j;
+        need = S.meta_host[j + 1];
+        break;
+      }
+    const double base = (double)(S.chunk + S.chunk / 4 + (1u << 20));
+    const double g = std::max(S.st[(size_t)k].grow * 2.0, 1.125 * (double)need / base);
+    for (int j = k; j < S.count; ++j) S.st[(size_t)j].grow = std::max(S.st[(size_t)j].grow, g);
+    if (attempt >= 2 * S.count + 8) return kErrUnknown;
+    e = cudaStreamSynchronize(S.d2h);  // out[] may be replaced
+    if (e == cudaSuccess) e = S.size_buffers();
+    if (e != cudaSuccess) return (int)e;
   }
+}
+
+int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+                   const int* rep_lens, int count, size_t chunk_bytes, uint8_t** out_host, size_t* out_len) {
+  crb::PinnedPool& pool = crb::host_pinned_pool();
+  Stream S;
+  for (int k = 0; k < count; ++k)
+    if (pat_lens[k] < 0 || rep_lens[k] < 0 || (pat_lens[k] && !pats[k]) || (rep_lens[k] && !reps[k])) return -1;
+  if (n == 0) {  // nothing matches in an empty input; the pairs must still be ones this path takes
+    for (int k = 0; k < count; ++k)
+      if (pat_lens[k] == 0 || pat_lens[k] > crb::kInlineMax || rep_lens[k] > crb::kInlineMax) return kUnsupported;
+    for (int k = 0; k < count; ++k) {
+      ReplaceParams q;
+      memset(&q, 0, sizeof(q));
+      crb::prepare_pattern_fields(q, pats[k], (uint32_t)pat_lens[k]);
+      if (!crb::super_nsub(q.mode, q.L)) return kUnsupported;
+    }
+    return 0;
+  }
+  const bool src_pinned = is_pinned(src);
+  const int src_rc = stream_setup(S, pats, pat_lens, reps, rep_lens, count,
+                                  std::max<size_t>(1, std::min(chunk_bytes ? chunk_bytes : (256u << 20), n)),
+                                  !src_pinned);
+  if (src_rc != 0) return src_rc;
+  cudaError_t e;
 
   // the result: page-locked, from the pool; grows by half when a chunk does not fit. One pair:
   // sized for the most matches it can keep (n / L of them), up to four times the input.
@@ -379,52 +443,7 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
     const int b = (int)(c & 1);
     const size_t m = std::min(S.chunk, n - c * S.chunk);
     const bool final = c + 1 == nchunks;
-    for (int attempt = 0;; ++attempt) {
-      e = cudaStreamWaitEvent(S.comp, S.ev_h2d[b], 0);
-      uint32_t e0 = 0;
-      if (e == cudaSuccess) e = S.run_chunk(b, m, c == 0, final, &e0);
-      if (e == cudaSuccess && attempt == 0 && !final) e = upload(c + 1);  // overlaps this chunk's stages
-      if (e == cudaSuccess) e = cudaStreamSynchronize(S.comp);
-      if (e != cudaSuccess) {
-        rc = (int)e;
-        break;
-      }
-      const ApplyResult r = *S.res_host;
-      const uint32_t e1 = e0 + (uint32_t)count - 1u;
-      if (r.error_epoch >= e0 && r.error_epoch <= e1) {
-        rc = kErrUnknown;  // a bounded wait in the kernel gave up
-        break;
-      }
-      if (r.overflow_epoch >= e0 && r.overflow_epoch <= e1) {
-        // The chunk's inputs (in0[b], pend[b], the carries of parity b) are intact: grow the
-        // buffer that overflowed and run the chunk again. The first stage whose output length
-        // passed its buffer is the one that overflowed (later stages read a clamped input);
-        // that length is exact, so one regrow per stage suffices.
-        int k = count - 1;
-        unsigned long long need = S.meta_host[count];
-        for (int j = 0; j + 1 < count; ++j)
-          if (S.meta_host[j + 1] > S.xcap) {
-            k = j;
-            need = S.meta_host[j + 1];
-            break;
-          }
-        const double base = (double)(S.chunk + S.chunk / 4 + (1u << 20));
-        const double g = std::max(S.st[(size_t)k].grow * 2.0, 1.125 * (double)need / base);
-        for (int j = k; j < count; ++j) S.st[(size_t)j].grow = std::max(S.st[(size_t)j].grow, g);
-        if (attempt >= 2 * count + 8) {
-          rc = kErrUnknown;
-          break;
-        }
-        e = cudaStreamSynchronize(S.d2h);  // out[] may be replaced
-        if (e == cudaSuccess) e = S.size_buffers();
-        if (e != cudaSuccess) {
-          rc = (int)e;
-          break;
-        }
-        continue;
-      }
-      break;
-    }
+    rc = run_chunk_fitting(S, b, m, c == 0, final, [&]() { return final ? cudaSuccess : upload(c + 1); });
     if (rc) break;
     const size_t olen = (size_t)S.meta_host[count];
     if (written + olen > ocap) {
@@ -473,7 +492,158 @@ int stream_replace(const uint8_t* src, size_t n, const uint8_t** pats, const int
   return 0;
 }
 
+// read() until m bytes are in or the input ends; the bytes read, or -1 on an error (errno set).
+long long read_full(int fd, uint8_t* dst, size_t m) {
+  size_t got = 0;
+  while (got < m) {
+    const ssize_t r = ::read(fd, dst + got, m - got);
+    if (r < 0) {
+      if (errno == EINTR) continue;
+      return -1;
+    }
+    if (r == 0) break;
+    got += (size_t)r;
+  }
+  return (long long)got;
+}
+
+bool write_full(int fd, const uint8_t* src, size_t m) {
+  size_t put = 0;
+  while (put < m) {
+    const ssize_t w = ::write(fd, src + put, m - put);
+    if (w < 0) {
+      if (errno == EINTR) continue;
+      return false;
+    }
+    put += (size_t)w;
+  }
+  return true;
+}
+
+// The chunk-major stream between two file descriptors: chunks are read into two page-locked
+// buffers (the next one while the current one is on the device), every pair is applied to a
+// chunk on the device, and each chunk's output is downloaded into one of two page-locked
+// buffers and written out while the next chunk computes. Neither the input nor the output is
+// held whole in memory, and the input may be a pipe (its end is found by reading ahead).
+int stream_fd(int in_fd, int out_fd, const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
+              const int* rep_lens, int count, size_t chunk_bytes, unsigned long long* in_bytes,
+              unsigned long long* out_bytes) {
+  crb::PinnedPool& pool = crb::host_pinned_pool();
+  Stream S;
+  int rc = stream_setup(S, pats, pat_lens, reps, rep_lens, count, chunk_bytes ? chunk_bytes : (256u << 20), true);
+  if (rc != 0) return rc;
+  uint8_t* obuf[2] = {nullptr, nullptr};
+  size_t ocap[2] = {0, 0};
+  unsigned long long tin = 0, tout = 0;
+  auto upload = [&](int b, size_t m) -> cudaError_t {
+    cudaError_t err = cudaStreamWaitEvent(S.h2d, S.ev_stage0[b], 0);  // in0[b] no longer read
+    if (err == cudaSuccess) err = cudaMemcpyAsync(S.in0[b] + S.st[0].P, S.hin[b], m, cudaMemcpyHostToDevice, S.h2d);
+    if (err == cudaSuccess) err = cudaEventRecord(S.ev_h2d[b], S.h2d);
+    return err;
+  };
+  long long m_cur = read_full(in_fd, S.hin[0], S.chunk);
+  if (m_cur < 0) return kIoError;
+  cudaError_t e = cudaSuccess;
+  int prev_b = -1;  // a downloaded chunk not written yet
+  size_t prev_len = 0;
+  bool io_fail = false;
+  auto flush_prev = [&]() -> cudaError_t {
+    if (prev_b < 0) return cudaSuccess;
+    const cudaError_t err = cudaEventSynchronize(S.ev_d2h[prev_b]);
+    if (err != cudaSuccess) return err;
+    if (prev_len && !write_full(out_fd, obuf[prev_b], prev_len)) io_fail = true;
+    prev_b = -1;
+    return cudaSuccess;
+  };
+  if (m_cur > 0) {
+    tin = (unsigned long long)m_cur;
+    e = upload(0, (size_t)m_cur);
+    if (e != cudaSuccess) rc = (int)e;
+  }
+  for (size_t c = 0; m_cur > 0 && rc == 0 && !io_fail; ++c) {
+    const int b = (int)(c & 1);
+    e = cudaEventSynchronize(S.ev_h2d[b ^ 1]);  // hin[b ^ 1] fed the previous chunk's upload
+    if (e != cudaSuccess) {
+      rc = (int)e;
+      break;
+    }
+    const long long m_next = read_full(in_fd, S.hin[b ^ 1], S.chunk);  // read ahead: is this the last?
+    if (m_next < 0) {
+      io_fail = true;
+      break;
+    }
+    const bool final = m_next == 0;
+    rc = run_chunk_fitting(S, b, (size_t)m_cur, c == 0, final, [&]() {
+      cudaError_t err = final ? cudaSuccess : upload(b ^ 1, (size_t)m_next);
+      if (err == cudaSuccess) err = flush_prev();  // the previous chunk's output, while this one computes
+      return err;
+    });
+    if (rc) break;
+    e = flush_prev();  // (a chunk that needed a rerun reached here without the write)
+    if (e != cudaSuccess) {
+      rc = (int)e;
+      break;
+    }
+    const size_t olen = (size_t)S.meta_host[count];
+    if (olen > ocap[b]) {
+      if (obuf[b]) pool.put(obuf[b]);
+      obuf[b] = static_cast<uint8_t*>(pool.get(olen + olen / 8, &e));
+      if (!obuf[b]) {
+        rc = (int)e;
+        break;
+      }
+      ocap[b] = olen + olen / 8;
+    }
+    if (olen) e = cudaMemcpyAsync(obuf[b], S.out[b], olen, cudaMemcpyDeviceToHost, S.d2h);
+    if (e == cudaSuccess) e = cudaEventRecord(S.ev_d2h[b], S.d2h);
+    if (e != cudaSuccess) {
+      rc = (int)e;
+      break;
+    }
+    prev_b = b;
+    prev_len = olen;
+    tout += olen;
+    m_cur = m_next;
+    tin += (unsigned long long)m_next;
+  }
+  if (rc == 0) {
+    e = flush_prev();
+    if (e != cudaSuccess) rc = (int)e;
+  }
+  cudaStreamSynchronize(S.d2h);
+  cudaStreamSynchronize(S.h2d);
+  for (int b = 0; b < 2; ++b)
+    if (obuf[b]) pool.put(obuf[b]);
+  if (rc == 0 && io_fail) rc = kIoError;
+  if (in_bytes) *in_bytes = tin;
+  if (out_bytes) *out_bytes = tout;
+  return rc;
+}
+
 }  // namespace
+
+CR_EXPORT int cuda_replace_stream_fd(int in_fd, int out_fd, const uint8_t** pats, const int* pat_lens,
+                                     const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
+                                     unsigned long long* in_bytes, unsigned long long* out_bytes) {
+  if (in_fd < 0 || out_fd < 0 || count < 0 || (count > 0 && (!pats || !pat_lens || !reps || !rep_lens))) return -1;
+  if (in_bytes) *in_bytes = 0;
+  if (out_bytes) *out_bytes = 0;
+  if (count == 0) {  // no pair: the output is the input
+    std::vector<uint8_t> buf((size_t)8 << 20);
+    unsigned long long total = 0;
+    for (;;) {
+      const long long m = read_full(in_fd, buf.data(), buf.size());
+      if (m < 0) return kIoError;
+      if (m == 0) break;
+      if (!write_full(out_fd, buf.data(), (size_t)m)) return kIoError;
+      total += (unsigned long long)m;
+    }
+    if (in_bytes) *in_bytes = total;
+    if (out_bytes) *out_bytes = total;
+    return 0;
+  }
+  return stream_fd(in_fd, out_fd, pats, pat_lens, reps, rep_lens, count, chunk_bytes, in_bytes, out_bytes);
+}
 
 CR_EXPORT int cuda_replace_stream(const uint8_t* src, size_t n, const uint8_t** pats, const int* pat_lens,
                                   const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,

@@ -107,7 +107,7 @@ class CudaReplaceLib:
                 f"{path} not found: build it with `python -m cuda_replace_b200.build` "
                 "(the replace path has no CPU fallback)")
         self.path = str(path)
-        self.lib = C.CDLL(self.path)
+        self.lib = C.CDLL(self.path, use_errno=True)
         lib = self.lib
         _bind(lib, "cuda_replace_unified",
               [c_uint8_p, c_size_t, c_uint8_p, C.c_int, c_uint8_p, C.c_int, C.POINTER(c_uint8_p), c_size_t_p],
@@ -157,6 +157,9 @@ class CudaReplaceLib:
               [C.c_int, c_uint8_pp, c_size_t_p, c_int_p, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p,
                c_uint8_pp, c_size_t_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_jobs_release", [], None, optional=True)
+        _bind(lib, "cuda_replace_stream_fd",
+              [C.c_int, C.c_int, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t,
+               C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)], C.c_int, optional=True)
         _bind(lib, "cuda_replace_plan_stages",
               [c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, C.c_int, c_int_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_host_copy", [c_void_p, c_void_p, c_size_t], None, optional=True)
@@ -518,6 +521,29 @@ def stream_native(lib: CudaReplaceLib, src, pairs: Sequence[Tuple[bytes, bytes]]
         return _bytes_at(out_ptr, out_len.value, lib.lib)
     finally:
         lib.lib.cuda_free_host(out_ptr)
+
+
+def stream_file(lib: CudaReplaceLib, in_fd: int, out_fd: int, pairs: Sequence[Tuple[bytes, bytes]],
+                chunk_bytes: int = 256 * 1024 * 1024) -> Tuple[int, int]:
+    """Chained replacement from one open file descriptor to another (cuda_replace_stream_fd):
+    chunk-major on the device, the input read and the output written piece by piece, so
+    neither is held whole in memory. Returns (bytes read, bytes written)."""
+    fn = getattr(lib.lib, "cuda_replace_stream_fd", None)
+    if fn is None:
+        raise RuntimeError("this libcuda_replace.so has no cuda_replace_stream_fd")
+    keep, pat_ptrs, pat_lens, rep_ptrs, rep_lens = _pair_arrays(pairs)
+    nin, nout = C.c_ulonglong(0), C.c_ulonglong(0)
+    rc = fn(C.c_int(in_fd), C.c_int(out_fd), C.cast(pat_ptrs, c_uint8_pp), C.cast(pat_lens, c_int_p),
+            C.cast(rep_ptrs, c_uint8_pp), C.cast(rep_lens, c_int_p), C.c_int(len(pairs)),
+            c_size_t(int(chunk_bytes)), C.byref(nin), C.byref(nout))
+    del keep
+    if rc == STREAM_UNSUPPORTED:
+        raise ValueError("a pair is outside the limits of the chunk-major stream")
+    if rc == -10:
+        raise OSError(C.get_errno(), "cuda_replace_stream_fd: reading or writing failed")
+    if rc != 0:
+        raise RuntimeError(f"cuda_replace_stream_fd failed rc={rc}")
+    return int(nin.value), int(nout.value)
 
 
 def _stream_supported(lib: CudaReplaceLib, pat: bytes, rep: bytes) -> bool:

@@ -207,6 +207,19 @@ int cuda_replace_stream(const uint8_t* src, size_t n, const uint8_t** pats, cons
 int cuda_replace_plan_stages(const uint8_t** pats, const int* pat_lens, const uint8_t** reps,
                              const int* rep_lens, int count, int keep_last_alone, int* stage_of);
 
+/* As cuda_replace_stream, between two open file descriptors (no counterpart in the reference,
+ * whose streaming helper takes and returns Python bytes, cuda_replace_wrapper.py:305-366): the
+ * input is read from in_fd until it ends (a regular file or a pipe) in chunk_bytes pieces (0 =
+ * 256 MiB) into two page-locked buffers, the next piece while the current one is on the
+ * device; each piece's output is written to out_fd while the next piece computes. Neither the
+ * input nor the output is ever held whole in host or device memory. *in_bytes / *out_bytes
+ * (may be NULL) receive the bytes read and written. Same pair limits as cuda_replace_stream
+ * (-7 outside them); -10 when reading or writing failed (errno tells why); -1 for invalid
+ * arguments; >0 a cudaError_t. On an error the output file holds a prefix of the result. */
+int cuda_replace_stream_fd(int in_fd, int out_fd, const uint8_t** pats, const int* pat_lens,
+                           const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
+                           unsigned long long* in_bytes, unsigned long long* out_bytes);
+
 /* Host memcpy on up to 8 threads (large copies): moves a result out of the page-locked
  * block the library returned into memory the caller allocated (in Python: a bytes object
  * created uninitialised), whose first-touch page faults bound a single-threaded copy. No
