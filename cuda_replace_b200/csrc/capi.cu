@@ -17,12 +17,14 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -165,6 +167,7 @@ struct Session {
   // unified() on a large page-locked input: upload and download streams, one event per chunk
   cudaStream_t up = nullptr, down = nullptr;
   cudaEvent_t ev_up[kUnifiedChunks] = {}, ev_done[kUnifiedChunks] = {};
+  cudaEvent_t ev_stage[3] = {};             // a pageable input's staging slots (chunked unified)
   unsigned int* carry2 = nullptr;           // device: carry into / out of the current chunk
   unsigned long long* olen_dev = nullptr;   // device: output end of the current chunk
 };
@@ -286,6 +289,8 @@ void session_free(Session* s) {
   if (s->pres) cudaFree(s->pres);
   if (s->mtab) cudaFree(s->mtab);
   if (s->mtab_host) cudaFreeHost(s->mtab_host);
+  for (int k = 0; k < 3; ++k)
+    if (s->ev_stage[k]) cudaEventDestroy(s->ev_stage[k]);
   for (int k = 0; k < kUnifiedChunks; ++k) {
     if (s->ev_up[k]) cudaEventDestroy(s->ev_up[k]);
     if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
@@ -1099,9 +1104,9 @@ CR_EXPORT void cuda_replace_close(void* h) {
 // single-launch path), else 0 or an error code (a cudaError_t, or 999).
 int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat, uint32_t L, const uint8_t* rep,
                     uint32_t R, uint8_t** out_host, size_t* out_len) {
-  if (n < kUnifiedChunkedMin || L == 0 || L > (uint32_t)crb::kInlineMax || R > (uint32_t)crb::kInlineMax ||
-      !host_is_pinned(src))
+  if (n < kUnifiedChunkedMin || L == 0 || L > (uint32_t)crb::kInlineMax || R > (uint32_t)crb::kInlineMax)
     return kFallback;
+  const bool pinned = host_is_pinned(src);
   ReplaceParams proto;
   memset(&proto, 0, sizeof(proto));
   crb::prepare_pattern_fields(proto, pat, L);
@@ -1141,16 +1146,68 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
     cudaGetLastError();  // a page-locked block of the worst case was refused: the single-launch
     return kFallback;            // path allocates the result at its exact size
   }
-  for (size_t k = 0; k < nchunks && e == cudaSuccess; ++k) {
-    const size_t a = bnd(k), m = bnd(k + 1) - a;
-    e = cudaMemcpyAsync(s->buf + a, src + a, m, cudaMemcpyHostToDevice, s->up);
-    if (e == cudaSuccess) e = cudaEventRecord(s->ev_up[k], s->up);
+  // Uploads. A page-locked input: every chunk's copy is queued at once. A pageable one: a
+  // producer thread copies each chunk (on the copy workers) into one of kStageSlots page-locked
+  // staging buffers and queues its upload from there, while this thread replaces and downloads
+  // the chunks already up; ready counts the chunks whose upload (and event) is queued.
+  constexpr int kStageSlots = 3;
+  uint8_t* stage[kStageSlots] = {};
+  std::mutex rmu;
+  std::condition_variable rcv;
+  size_t ready = 0;
+  cudaError_t prod_err = cudaSuccess;
+  std::atomic<bool> stop{false};
+  std::thread producer;
+  if (pinned) {
+    for (size_t k = 0; k < nchunks && e == cudaSuccess; ++k) {
+      const size_t a = bnd(k), m = bnd(k + 1) - a;
+      e = cudaMemcpyAsync(s->buf + a, src + a, m, cudaMemcpyHostToDevice, s->up);
+      if (e == cudaSuccess) e = cudaEventRecord(s->ev_up[k], s->up);
+    }
+    ready = nchunks;
+  } else {
+    for (int i = 0; i < kStageSlots && e == cudaSuccess; ++i) {
+      if (!s->ev_stage[i]) e = cudaEventCreateWithFlags(&s->ev_stage[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) stage[i] = static_cast<uint8_t*>(pinned_pool().get(chunk + P, &e));
+    }
+    if (e == cudaSuccess) {
+      const int dev = s->device;
+      producer = std::thread([&, dev]() {
+        cudaSetDevice(dev);
+        cudaError_t pe = cudaSuccess;
+        for (size_t k = 0; k < nchunks && pe == cudaSuccess && !stop.load(); ++k) {
+          const int slot = (int)(k % kStageSlots);
+          const size_t a = bnd(k), m = bnd(k + 1) - a;
+          if (k >= (size_t)kStageSlots) pe = cudaEventSynchronize(s->ev_stage[slot]);  // the slot's upload is done
+          if (pe != cudaSuccess) break;
+          crb::parallel_memcpy(stage[slot], src + a, m);
+          pe = cudaMemcpyAsync(s->buf + a, stage[slot], m, cudaMemcpyHostToDevice, s->up);
+          if (pe == cudaSuccess) pe = cudaEventRecord(s->ev_up[k], s->up);
+          if (pe == cudaSuccess) pe = cudaEventRecord(s->ev_stage[slot], s->up);
+          std::lock_guard<std::mutex> g(rmu);
+          if (pe == cudaSuccess) ready = k + 1;
+          prod_err = pe;
+          rcv.notify_all();
+        }
+        std::lock_guard<std::mutex> g(rmu);
+        if (pe != cudaSuccess) prod_err = pe;
+        rcv.notify_all();
+      });
+    }
   }
   int rc = (int)e;
   size_t O = 0;
   for (size_t k = 0; k < nchunks && rc == 0; ++k) {
     const size_t a = bnd(k), m = bnd(k + 1) - a;
     const bool first = k == 0, final = k + 1 == nchunks;
+    if (!pinned) {  // wait until the producer has queued this chunk's upload
+      std::unique_lock<std::mutex> lk(rmu);
+      rcv.wait(lk, [&] { return ready > k || prod_err != cudaSuccess; });
+      if (ready <= k) {
+        rc = (int)prod_err;
+        break;
+      }
+    }
     const size_t held = first ? 0 : P;  // the previous chunk's last bytes, matched again here
     ReplaceParams p = proto;
     p.in = s->buf + (a - held);  // k * chunk: 16-byte aligned
@@ -1198,10 +1255,14 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
     }
     O += olen;
   }
+  stop.store(true);
+  if (producer.joinable()) producer.join();
   const cudaError_t e1 = cudaStreamSynchronize(s->down);
   const cudaError_t e2 = cudaStreamSynchronize(s->up);
   if (rc == 0 && e1 != cudaSuccess) rc = (int)e1;
   if (rc == 0 && e2 != cudaSuccess) rc = (int)e2;
+  for (int i = 0; i < kStageSlots; ++i)
+    if (stage[i]) pinned_pool().put(stage[i]);  // its uploads finished with the stream above
   s->len = 0;  // the session's buffers hold no complete content now
   ++s->buf_version;
   s->q_kind = 0;

@@ -48,8 +48,9 @@ extern "C" {
 const char* cuda_replace_version(void);
 
 /* One-shot replace: upload src, replace every leftmost non-overlapping pat with rep,
- * return the result in library-owned page-locked memory. A page-locked src of 256 MiB or
- * more is uploaded, replaced and downloaded chunk by chunk, the directions overlapped.
+ * return the result in library-owned page-locked memory. A src of 256 MiB or more is uploaded,
+ * replaced and downloaded chunk by chunk, the directions overlapped (a pageable src is copied
+ * chunk by chunk into page-locked staging buffers by a second host thread meanwhile).
  * Replaces cuda_replace_unified (cuda_replace.cu:2579);
  * bound at cuda_replace_wrapper.py:48-54, called at cuda_replace_wrapper.py:124-141. */
 int cuda_replace_unified(const uint8_t* src, size_t src_len,

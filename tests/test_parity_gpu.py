@@ -163,8 +163,9 @@ def test_large_inputs_unified_and_stream(cr_lib):
 
 
 def test_unified_page_locked_large_chunked(cr_lib):
-    """unified() on a page-locked input of 256 MiB or more takes the chunked path (uploads,
-    replaces and downloads of up to sixteen chunks overlapped): results equal bytes.replace, also
+    """unified() on an input of 256 MiB or more takes the chunked path (uploads, replaces and
+    downloads of up to sixteen chunks overlapped; a pageable input staged chunk by chunk through
+    page-locked buffers by a producer thread): results equal bytes.replace, also
     for matches planted across every chunk join, for bordered and free patterns, expansion and
     deletion."""
     import ctypes as C
@@ -189,9 +190,11 @@ def test_unified_page_locked_large_chunked(cr_lib):
     for src, cases in ((text, ((b"&amp;", b"&"), (b"&amp;", b"<e>"), (b"abab", b"X"), (b"\x00", b""))),
                        (run, ((b"aa", b"X"), (b"a", b"bcd"), (b"aaa", b"")))):
         h = torch.frombuffer(bytearray(src), dtype=torch.uint8).pin_memory()
-        for pat, rep in cases:
+        # page-locked (every upload queued at once) and pageable (staged by a producer thread)
+        for pinned, pat, rep in [(True, pt, rp) for pt, rp in cases] + [(False, pt, rp) for pt, rp in cases[:2]]:
+            ptr = C.cast(h.data_ptr(), C.POINTER(C.c_uint8)) if pinned else C.cast(C.c_char_p(src), C.POINTER(C.c_uint8))
             pb, rb = C.create_string_buffer(pat, len(pat)), C.create_string_buffer(rep, len(rep) or 1)
-            rc = cr_lib.lib.cuda_replace_unified(C.cast(h.data_ptr(), C.POINTER(C.c_uint8)), n,
+            rc = cr_lib.lib.cuda_replace_unified(ptr, n,
                                                  C.cast(pb, C.POINTER(C.c_uint8)), len(pat),
                                                  C.cast(rb, C.POINTER(C.c_uint8)), len(rep),
                                                  C.byref(out_ptr), C.byref(out_len))
