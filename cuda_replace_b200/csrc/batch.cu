@@ -565,13 +565,22 @@ class Engine {
     for (int i = 0; i < nj && e == cudaSuccess; ++i)
       e = cudaMemcpy(buf + (size_t)i * 2 * (n + 4096), host.data(), n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = s.ensure_tiles((size_t)nj * (n / crb::kTile + 2));
-    // one representative pair per class: borderless L = 4; bordered L = 2; bordered L = 8
-    const uint8_t p0[4] = {'a', 'b', 'c', 'd'}, p1[2] = {'a', 'a'}, p2[8] = {'a', 'b', 'a', 'c', 'a', 'b', 'a', 'b'};
+    // two representative pairs per class, at the short and the long end of its pattern
+    // lengths (the candidate test and the tables cost differently there): borderless L = 2 and
+    // L = 12; bordered L = 2 and L = 4; bordered L = 6 and L = 24
+    const uint8_t p0[4] = {'a', 'b', 'c', 'd'}, p0b[12] = {'a', 'b', 'c', 'd', 'e', 'f', 'g', 'h', 'i', 'j', 'k', 'l'};
+    const uint8_t p1[2] = {'a', 'a'}, p1b[4] = {'a', 'b', 'a', 'b'};
+    const uint8_t p2[6] = {'a', 'b', 'c', 'a', 'b', 'c'};
+    uint8_t p2b[24];
+    for (int i = 0; i < 24; ++i) p2b[i] = (uint8_t)("abac"[i % 4]);
     const uint8_t rp[8] = {'X', 'Y', 'Z', 'W', 'V', 'U', 'T', 'S'};
-    SegPair q[kClasses];
-    crb::make_seg_pair(q[0], p0, 4, rp, 6);
-    crb::make_seg_pair(q[1], p1, 2, rp, 1);
-    crb::make_seg_pair(q[2], p2, 8, rp, 3);
+    SegPair q[kClasses][2];
+    crb::make_seg_pair(q[0][0], p0, 2, rp, 6);
+    crb::make_seg_pair(q[0][1], p0b, 12, rp, 3);
+    crb::make_seg_pair(q[1][0], p1, 2, rp, 1);
+    crb::make_seg_pair(q[1][1], p1b, 4, rp, 2);
+    crb::make_seg_pair(q[2][0], p2, 6, rp, 3);
+    crb::make_seg_pair(q[2][1], p2b, 24, rp, 5);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -582,7 +591,13 @@ class Engine {
       if (c == 2) cands = {1u, 2u, 4u};
       float best = 1e30f;
       ClassCfg pick;
-      for (uint32_t ns : cands) {
+      // super-tile size x CTAs per SM (the full occupancy, one less, half), each timed on both
+      // representative pairs; the sum decides
+      for (uint32_t ns : cands)
+      for (int occ_step = 0; occ_step < 3 && e == cudaSuccess; ++occ_step) {
+      float tot = 0;
+      int grid = 0;
+      for (int qv = 0; qv < 2 && e == cudaSuccess; ++qv) {
         memset(s.h_njobs, 0, kMaxRounds * kClasses * sizeof(unsigned int));
         s.h_njobs[c] = (unsigned int)nj;
         std::vector<unsigned long long> hl((size_t)nj * 2, 0);
@@ -598,7 +613,7 @@ class Engine {
           J.res = (unsigned int)i;
           hl[(size_t)2 * i] = n;
         }
-        s.h_pairs[0] = q[c];
+        s.h_pairs[0] = q[c][qv];
         Tuning tu = tune;
         tu.cls[c].nsub = ns;
         SegLaunch sl = s.launch_desc(0, c, tu);
@@ -607,7 +622,12 @@ class Engine {
           e = cudaErrorUnknown;
           break;
         }
-        const int grid = per_sm * sms;
+        const int occ = occ_step == 0 ? per_sm : (occ_step == 1 ? per_sm - 1 : per_sm / 2);
+        if (occ < 1 || (occ_step == 2 && occ == per_sm - 1)) {
+          tot = 1e30f;  // not a distinct candidate
+          break;
+        }
+        grid = occ * sms;
         e = cudaMemcpy(lens, hl.data(), hl.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
           e = cudaMemcpy(s.d_jobs + (size_t)c * s.max_jobs, s.h_jobs + (size_t)c * s.max_jobs, nj * sizeof(SegJob),
@@ -615,7 +635,6 @@ class Engine {
         if (e == cudaSuccess)
           e = cudaMemcpy(s.d_njobs, s.h_njobs, kMaxRounds * kClasses * sizeof(unsigned int), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(s.d_pairs, s.h_pairs, sizeof(SegPair), cudaMemcpyHostToDevice);
-        float tot = 0;
         for (int it = 0; it < 4 && e == cudaSuccess; ++it) {
           e = cudaMemsetAsync(s.d_res, 0, (size_t)nj * sizeof(ApplyResult), s.st);
           if (e == cudaSuccess) e = cudaEventRecord(e0, s.st);
@@ -626,12 +645,13 @@ class Engine {
           if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
           if (it > 0) tot += ms;  // the first run warms up
         }
+      }
         if (e != cudaSuccess) break;
         if (tot < best) {
           best = tot;
           pick.nsub = ns;
           pick.grid = grid;
-          pick.us = tot / 3.0f * 1000.0f;
+          pick.us = tot / 6.0f * 1000.0f;
         }
       }
       tune.cls[c] = pick;
