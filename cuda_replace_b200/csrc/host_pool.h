@@ -29,8 +29,9 @@ class PinnedPool {
       std::lock_guard<std::mutex> g(mu_);
       auto it = idle_.lower_bound(want);
       if (it != idle_.end() && it->first <= want + want / 2 + (64ull << 20)) {
-        void* p = it->second;
+        void* p = it->second.first;
         idle_bytes_ -= it->first;
+        lru_.erase(it->second.second);
         idle_.erase(it);
         *err = cudaSuccess;
         return p;
@@ -43,6 +44,8 @@ class PinnedPool {
     sizes_[p] = want;
     return p;
   }
+  // Keep p for reuse. Over kMaxIdle idle bytes, the blocks idle the longest are released first
+  // (so a large block handed back, the one most likely wanted again soon, is kept).
   void put(void* p) {
     if (!p) return;
     std::vector<void*> evict;
@@ -52,14 +55,25 @@ class PinnedPool {
       if (s == sizes_.end()) {
         evict.push_back(p);  // not ours: release directly
       } else {
-        idle_.emplace(s->second, p);
+        const unsigned long long seq = ++seq_;
+        idle_.emplace(s->second, std::make_pair(p, seq));
+        lru_.emplace(seq, std::make_pair(s->second, p));
         idle_bytes_ += s->second;
-        while (idle_bytes_ > kMaxIdle && !idle_.empty()) {
-          auto big = std::prev(idle_.end());
-          idle_bytes_ -= big->first;
-          sizes_.erase(big->second);
-          evict.push_back(big->second);
-          idle_.erase(big);
+        while (idle_bytes_ > kMaxIdle && !lru_.empty()) {
+          auto old = lru_.begin();
+          if (old->first == seq && lru_.size() > 1) old = std::next(old);  // not the block just returned
+          const size_t sz = old->second.first;
+          void* q = old->second.second;
+          auto range = idle_.equal_range(sz);
+          for (auto it = range.first; it != range.second; ++it)
+            if (it->second.first == q) {
+              idle_.erase(it);
+              break;
+            }
+          idle_bytes_ -= sz;
+          sizes_.erase(q);
+          evict.push_back(q);
+          lru_.erase(old);
         }
       }
     }
@@ -69,9 +83,11 @@ class PinnedPool {
  private:
   static constexpr size_t kMaxIdle = 24ull << 30;
   std::mutex mu_;
-  std::multimap<size_t, void*> idle_;
+  std::multimap<size_t, std::pair<void*, unsigned long long>> idle_;  // size -> (block, put order)
+  std::map<unsigned long long, std::pair<size_t, void*>> lru_;        // put order -> (size, block)
   std::unordered_map<void*, size_t> sizes_;
   size_t idle_bytes_ = 0;
+  unsigned long long seq_ = 0;
 };
 
 // The process-wide pool (never destroyed: CUDA may be torn down first at exit).
@@ -118,7 +134,7 @@ class CopyWorkers {
  private:
   CopyWorkers() {
     const unsigned hw = std::thread::hardware_concurrency();
-    nthreads_ = hw > 1 ? (hw - 1 < 7u ? hw - 1 : 7u) : 0u;
+    nthreads_ = hw > 1 ? (hw - 1 < 15u ? hw - 1 : 15u) : 0u;
     for (unsigned i = 0; i < nthreads_; ++i) std::thread([this] { loop(); }).detach();
   }
   void loop() {

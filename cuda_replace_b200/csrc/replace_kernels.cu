@@ -1018,14 +1018,7 @@ namespace {
 
 constexpr int kNBuf = 2;
 constexpr int kMaxSub = 8;
-#ifndef CRB_CLAIM_AHEAD
-#define CRB_CLAIM_AHEAD 0
-#endif
-constexpr bool kClaimAhead = CRB_CLAIM_AHEAD != 0;
-#ifndef CRB_PASSB_DIRECT
-#define CRB_PASSB_DIRECT 0
-#endif
-constexpr bool kPassBDirect = CRB_PASSB_DIRECT != 0;
+
 
 struct LayoutS {
   uint32_t in0, outb, masks, pat, rep, tab16, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
@@ -1989,55 +1982,6 @@ __device__ __forceinline__ void warp_emit_literal(uint8_t* out, const uint8_t* t
   if (ok) out[b] = tb[srcw + (uint32_t)(b - g0)];
 }
 
-// 16 input bytes from global memory (read-only for the whole launch; the lines are in L2 since
-// pass A), letting L2 evict them first.
-__device__ __forceinline__ uint4 ld_in16(const uint8_t* src) {
-  uint4 v;
-  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "l"(src), "l"(l2_policy_evict_first()));
-  return v;
-}
-
-// warp_emit_literal with the source read from global memory: sub-tile bytes at src_g (16-byte
-// aligned), the region's first byte at src_g + srcw. A chunk reads the aligned 16 bytes holding
-// its first byte and, when it is not aligned, the next 16 (all of whose bytes it copies lie in
-// the region, so both reads stay inside the input).
-__device__ __forceinline__ void warp_emit_literal_g(uint8_t* out, const uint8_t* src_g, unsigned long long g0,
-                                                    uint32_t wtot, uint32_t srcw) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const unsigned long long ga = g0 & ~15ull;
-  const unsigned long long gend = g0 + wtot;
-  const uint32_t c0 = (uint32_t)((g0 - ga + 15ull) >> 4);
-  const uint32_t c1 = (uint32_t)((gend - ga) >> 4);
-  const uint32_t off0 = srcw + (uint32_t)(ga + ((unsigned long long)c0 << 4) - g0);
-  const uint32_t r = off0 & 15u, q = r >> 2, sh = (r & 3u) * 8u;
-  uint32_t c = c0 + lane;
-  for (; c + 32u < c1; c += 64u) {  // two chunks per lane in flight
-    const uint32_t a0 = off0 - r + ((c - c0) << 4), a1 = a0 + 512u;
-    const uint4 A0 = ld_in16(src_g + a0), A1 = ld_in16(src_g + a1);
-    const uint4 B0 = r ? ld_in16(src_g + a0 + 16u) : A0, B1 = r ? ld_in16(src_g + a1 + 16u) : A1;
-    st_out16(out + ga + ((unsigned long long)c << 4), extract16(A0, B0, q, sh));
-    st_out16(out + ga + ((unsigned long long)(c + 32u) << 4), extract16(A1, B1, q, sh));
-  }
-  for (; c < c1; c += 32u) {
-    const uint32_t a = off0 - r + ((c - c0) << 4);
-    const uint4 A = ld_in16(src_g + a);
-    const uint4 B = r ? ld_in16(src_g + a + 16u) : A;
-    st_out16(out + ga + ((unsigned long long)c << 4), extract16(A, B, q, sh));
-  }
-  unsigned long long b;
-  bool ok;
-  if (c0 < c1) {
-    b = lane < 16u ? g0 + lane : ga + ((unsigned long long)c1 << 4) + (lane - 16u);
-    ok = lane < 16u ? (b < ga + ((unsigned long long)c0 << 4)) : (b < gend);
-  } else {
-    b = g0 + lane;
-    ok = b < gend;
-  }
-  if (ok) out[b] = src_g[srcw + (uint32_t)(b - g0)];
-}
-
 // x mod R for x < 2^26 and 1 <= R <= 64, with rmag = ceil(2^32 / R) (0 for R = 1): the
 // quotient is the high word of x * rmag (its error, below x / 2^32, stays under 1/R).
 __host__ __device__ __forceinline__ uint32_t mod_magic(uint32_t R) {
@@ -2527,11 +2471,9 @@ __global__ void __launch_bounds__(kThreads, 3)
     s_q[0] = nx;
     if (nx != kNone) ring.push(nx, 0);
   };
-  auto schedule = [&](const uint32_t tcur, const uint32_t cset, const bool claimed) {
-    if (!claimed) claim_next();
-    // pass B reloads the sub-tiles into shared memory only in its general mode (and, without
-    // kPassBDirect, for the copies of the table-driven mode 2)
-    if (kPassBDirect ? s_noin[cset] == 0u : s_noin[cset] != 1u) ring.push(tcur, 1);
+  auto schedule = [&](const uint32_t tcur, const uint32_t cset) {
+    claim_next();
+    if (s_noin[cset] != 1u) ring.push(tcur, 1);
     ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
   };
 
@@ -2550,13 +2492,6 @@ __global__ void __launch_bounds__(kThreads, 3)
     uint8_t* const subrec_b = smem + lay.subrec + set * lay.subrec_set;
     const bool use_rec = kFreeLike || L <= 4u;
     const uint32_t tag = p.epoch & 0xFFFFFFu;
-    // With kClaimAhead the next super-tile is claimed and its pass-A loads queued before this
-    // look-back, so they stream in while the look-back waits.
-    const bool claim_ahead = kClaimAhead && tid == 0 && tnext != kNone;
-    if (claim_ahead) {
-      claim_next();
-      ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
-    }
     // ================= look back, publish the inclusive prefix
     if (warp == 0) {
       unsigned long long K = 0;
@@ -2607,7 +2542,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
     __syncthreads();
-    if (tid == 0 && tnext != kNone) schedule(tnext, nset, claim_ahead);
+    if (tid == 0 && tnext != kNone) schedule(tnext, nset);
     const uint32_t pbm = s_noin[set];  // pass B mode
     const bool noin = pbm == 1u;
     const uint32_t cin = s_cin;
@@ -2705,31 +2640,22 @@ __global__ void __launch_bounds__(kThreads, 3)
       if (odd && tid == 0) set_error(p);
       const bool write = fits_t && !odd && !failed;
       for (uint32_t j = 0; j < m; ++j) {
-        // kPassBDirect: copies read the input straight from global memory (L2), so this pass
-        // takes no load-ring slot and no barrier, and the next super-tile's loads keep the ring
-        const uint8_t* tb = kPassBDirect ? nullptr : ring.wait(p, smem, lay, s_bar, &s_fail);
+        const uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
         const uint32_t r = j * kWarps + warp;
         const uint32_t ol = __shfl_sync(0xffffffffu, olen_r, r);
         const uint32_t of = __shfl_sync(0xffffffffu, offr, r);
         const uint32_t cr = __shfl_sync(0xffffffffu, wc, r);
         const uint32_t xr = __shfl_sync(0xffffffffu, x0, r);
         if (write && ol) {
-          if (cr == 0u) {
-            if (kPassBDirect)
-              warp_emit_literal_g(p.out, p.in + tstart + (unsigned long long)j * kTile, O + of, ol,
-                                  warp * 2048u + xr);
-            else
-              warp_emit_literal(p.out, tb, O + of, ol, warp * 2048u + xr);
-          } else {
+          if (cr == 0u)
+            warp_emit_literal(p.out, tb, O + of, ol, warp * 2048u + xr);
+          else
             warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, rmag,
                               O + of, ol);
-          }
         }
-        if (!kPassBDirect) {
-          __syncthreads();
-          ring.release();
-          if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
-        }
+        __syncthreads();
+        ring.release();
+        if (tid == 0) ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
       }
       O += total;
     }
@@ -3189,7 +3115,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         tile_back(tprev, (k & 1u) ^ 1u, tcur, k & 1u);
       } else if (tcur != kNone) {
         __syncthreads();  // the fold's flags of tcur are visible to thread 0
-        if (tid == 0) schedule(tcur, k & 1u, false);
+        if (tid == 0) schedule(tcur, k & 1u);
       }
       tprev = tcur;
       ++k;

@@ -221,7 +221,7 @@ int cuda_replace_stream_fd(int in_fd, int out_fd, const uint8_t** pats, const in
                            const uint8_t** reps, const int* rep_lens, int count, size_t chunk_bytes,
                            unsigned long long* in_bytes, unsigned long long* out_bytes);
 
-/* Host memcpy on up to 8 threads (large copies): moves a result out of the page-locked
+/* Host memcpy on up to 16 threads (large copies): moves a result out of the page-locked
  * block the library returned into memory the caller allocated (in Python: a bytes object
  * created uninitialised), whose first-touch page faults bound a single-threaded copy. No
  * counterpart in the reference. */
