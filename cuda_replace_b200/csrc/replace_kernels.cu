@@ -1023,7 +1023,7 @@ constexpr int kMaxSub = 8;
 struct LayoutS {
   uint32_t in0, outb, masks, pat, rep, tab16, segtab, srec, wtab, wrec, subrec, total;  // buffer b at in0 + b * inbytes
   uint32_t masks_set, srec_set, wtab_set, wrec_set, subrec_set;  // bytes of one set of per-super-tile tables
-  uint32_t mtab, tinfo, tinfo_set;  // kModeMulti: the stage's pair table; per-thread (D, last match end)
+  uint32_t mtab;                    // kModeMulti: the stage's pair table
   uint32_t rs, inbytes;
   uint32_t wstage_words;  // padded staging words per warp (its 2 KiB of input may grow 3x)
   uint32_t wstage_cap;    // bytes one warp can stage (before the padding words)
@@ -1084,9 +1084,6 @@ __host__ __device__ __forceinline__ LayoutS make_layout_s(uint32_t mode, uint32_
   if (mode == kModeMulti) {
     s.mtab = off;
     off += align_up_u32((uint32_t)sizeof(MultiTable), 16);
-    s.tinfo = off;
-    s.tinfo_set = nsub * kThreads * 4u;
-    off += sets * s.tinfo_set;
   }
   s.total = off;
   return s;
@@ -2256,8 +2253,6 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         mask = kept;
         masks_s[j * kThreads + tid] = mask;
-        reinterpret_cast<uint32_t*>(smem + lay.tinfo + set * lay.tinfo_set)[j * kThreads + tid] =
-            ((uint32_t)dsum & 0xFFFFu) | (lastend << 16);
         const uint32_t cnt = __reduce_add_sync(0xffffffffu, (uint32_t)__popcll(mask));
         const int wd = __reduce_add_sync(0xffffffffu, dsum);
         const uint32_t cend = __reduce_max_sync(0xffffffffu, mask ? sb + lastend : 0u);
@@ -2757,15 +2752,23 @@ __global__ void __launch_bounds__(kThreads, 3)
       uint32_t tinf = 0;  // kModeMulti: this thread's (sum of R - L, last match end)
       if (!done) {
       if constexpr (MODE == kModeMulti) {
-        // only the previous segment's last match (or the sub-tile carry) can reach here (L <= 32)
-        const uint32_t* tinfo = reinterpret_cast<const uint32_t*>(smem + lay.tinfo + set * lay.tinfo_set);
-        tinf = tinfo[j * kThreads + tid];
-        uint32_t cov = tid == 0 ? csub_in : 0u;
-        if (tid > 0) {
-          const uint32_t e = tinfo[j * kThreads + tid - 1] >> 16;
-          if (e > 64u) cov = e - 64u;
+        // this thread's matches again (the pattern at each kept start): the sum of their R - L and
+        // where the last one ends; the carry into the segment is the previous thread's last match
+        // (L <= 32), or for a warp's first thread the carry into its region
+        int dsum = 0;
+        uint32_t le = 0;
+        for (uint64_t km = kept; km; km &= km - 1ull) {
+          const uint32_t b = (uint32_t)(__ffsll((long long)km) - 1);
+          const int k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
+          if (k >= 0) {
+            dsum += (int)MT.R[k] - (int)MT.L[k];
+            le = b + MT.L[k];
+          }
         }
-        x_in = cov;
+        tinf = ((uint32_t)dsum & 0xFFFFu) | (le << 16);
+        const uint32_t prev_le = __shfl_up_sync(0xffffffffu, le, 1);
+        const uint32_t pw = __shfl_sync(0xffffffffu, covs_l, warp);
+        x_in = lane == 0 ? (pw > sb ? pw - sb : 0u) : (prev_le > 64u ? prev_le - 64u : 0u);
       } else if (MODE == kModeFree) {
         if (L <= 64u) {
           // only the previous segment's last match (or the sub-tile carry) can reach here
@@ -2871,6 +2874,64 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
       } else if (fits && !failed && warp_stage) {
         if (len_ok) {
+        bool pieces_done = false;
+        if constexpr (MODE == kModeMulti) {
+          // Few matches in the region: its output is literal runs between replacements. Each
+          // run is copied by the whole warp (aligned 16-byte stores, like a copy-only region),
+          // each replacement by as many lanes as it has bytes; no staging of the whole output.
+          const uint32_t M = __reduce_add_sync(0xffffffffu, cnt);
+          if (M <= 16u) {
+            uint32_t* desc = reinterpret_cast<uint32_t*>(ob) + (size_t)warp * lay.wstage_words;
+            const uint32_t mb = warp_incl_scan(cnt, OpSum()) - cnt;  // this lane's first match index
+            uint32_t i = 0;
+            for (uint64_t km = kept; km; km &= km - 1ull, ++i) {
+              const uint32_t b = (uint32_t)(__ffsll((long long)km) - 1);
+              const int k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
+              desc[2 * (mb + i)] = lane * 64u + b;  // start within the region
+              desc[2 * (mb + i) + 1] = (uint32_t)(k < 0 ? 0 : k);
+            }
+            __syncwarp();
+            const uint32_t x0r = __shfl_sync(0xffffffffu, x_in, 0);  // covered at the region start
+            const uint32_t vend = __reduce_add_sync(0xffffffffu, V);  // input bytes of the region
+            // piece j (lane j <= M): the literal run before match j (after the last match for j = M)
+            uint32_t lstart = 0, llen = 0, rlen = 0, pid = 0;
+            if (lane <= M) {
+              uint32_t st0 = x0r;
+              if (lane > 0) {
+                const uint32_t pk = desc[2 * (lane - 1) + 1];
+                st0 = desc[2 * (lane - 1)] + MT.L[pk];
+              }
+              const uint32_t en = lane < M ? desc[2 * lane] : vend;
+              lstart = st0;
+              llen = en > st0 ? en - st0 : 0u;
+              if (lane < M) {
+                pid = desc[2 * lane + 1];
+                rlen = MT.R[pid];
+              }
+            }
+            const uint32_t piece = llen + rlen;
+            const uint32_t poff = warp_incl_scan(piece, OpSum()) - piece;
+            const unsigned long long g0 = O + wbase;
+            // the pieces fill exactly the region's slot (the same sum as the threads' lengths);
+            // otherwise nothing is written and the launch reports an error
+            const bool pieces_ok = __shfl_sync(0xffffffffu, poff + piece, 31) == wtot;
+            if (!pieces_ok && lane == 0) set_error(p);
+            for (uint32_t jp = 0; pieces_ok && jp <= M; ++jp) {
+              const uint32_t ls = __shfl_sync(0xffffffffu, lstart, jp);
+              const uint32_t ll = __shfl_sync(0xffffffffu, llen, jp);
+              const uint32_t po = __shfl_sync(0xffffffffu, poff, jp);
+              if (ll) warp_emit_literal(p.out, tb, g0 + po, ll, warp * 2048u + ls);
+              if (jp < M) {
+                const uint32_t rl = __shfl_sync(0xffffffffu, rlen, jp);
+                const uint32_t pk = __shfl_sync(0xffffffffu, pid, jp);
+                for (uint32_t q = lane; q < rl; q += 32u) p.out[g0 + po + ll + q] = MT.rep[pk][q];
+              }
+            }
+            __syncwarp();
+            pieces_done = true;
+          }
+        }
+        if (!pieces_done) {
         uint32_t W[17];
         load_seg_words(tb + sb, W);
         // ---- this warp's output: assemble in its padded staging area, then copy out
@@ -2959,6 +3020,7 @@ __global__ void __launch_bounds__(kThreads, 3)
             p.out[b] = sbytes[stg_pad(sbi >> 2) * 4u + (sbi & 3u)];
           }
         }
+        }  // !pieces_done
         }  // len_ok
       } else if (fits && !failed) {
         // very large expansions: windows of the sub-tile output, byte by byte (the windows
