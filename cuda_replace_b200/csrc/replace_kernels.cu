@@ -1200,6 +1200,42 @@ __device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t 
       return mask;
     }
   }
+  if (L >= 2u && ((p4 >> 8) & 0xFFu) != b0) {
+    // Positions of the first byte, kept in a transposed order that costs fewer operations:
+    // bit 8j + i of t0 (t1) is byte j of rotated word i (i + 8). ~((((w ^ rep) & 0x7f..) +
+    // 0x7f..) | (w ^ rep)) has bit 7 of a byte set exactly when the byte equals b0; a shift
+    // moves those bits to 8j + i and a masked OR adds them.
+    uint32_t t0 = 0, t1 = 0;
+#define CRB_FIRST_BYTE(word, acc, i)                                                 \
+    {                                                                                \
+      const uint32_t x_ = (word) ^ rep;                                              \
+      const uint32_t f_ = ~(((x_ & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x_);                \
+      acc |= (f_ >> (7u - (i))) & (0x01010101u << (i));                              \
+    }
+    CRB_FIRST_BYTE(q0.x, t0, 0u) CRB_FIRST_BYTE(q0.y, t0, 1u) CRB_FIRST_BYTE(q0.z, t0, 2u) CRB_FIRST_BYTE(q0.w, t0, 3u)
+    CRB_FIRST_BYTE(q1.x, t0, 4u) CRB_FIRST_BYTE(q1.y, t0, 5u) CRB_FIRST_BYTE(q1.z, t0, 6u) CRB_FIRST_BYTE(q1.w, t0, 7u)
+    CRB_FIRST_BYTE(q2.x, t1, 0u) CRB_FIRST_BYTE(q2.y, t1, 1u) CRB_FIRST_BYTE(q2.z, t1, 2u) CRB_FIRST_BYTE(q2.w, t1, 3u)
+    CRB_FIRST_BYTE(q3.x, t1, 4u) CRB_FIRST_BYTE(q3.y, t1, 5u) CRB_FIRST_BYTE(q3.z, t1, 6u) CRB_FIRST_BYTE(q3.w, t1, 7u)
+#undef CRB_FIRST_BYTE
+    if (__any_sync(0xffffffffu, __popc(t0) + __popc(t1) > 12)) {
+      uint32_t w[17];
+      load_seg_words(seg, w);
+      return candidates_from_words(w, p4, m4);
+    }
+    uint64_t out = 0;
+    for (int h = 0; h < 2; ++h) {
+      uint32_t m = h ? t1 : t0;
+      while (m) {
+        const uint32_t b = (uint32_t)(__ffs(m) - 1);
+        m &= m - 1u;
+        const uint32_t i = (b & 7u) + 8u * (uint32_t)h;                    // rotated word
+        const uint32_t nat = (((rot + (i >> 2)) & 3u) << 2) | (i & 3u);  // natural word
+        const uint32_t pos = 4u * nat + (b >> 3);
+        if (((ld_u32_unaligned(seg + pos) ^ p4) & m4) == 0u) out |= 1ull << pos;
+      }
+    }
+    return out;
+  }
   const uint32_t lo = eq_nibble(q0.x, rep) | (eq_nibble(q0.y, rep) << 4) | (eq_nibble(q0.z, rep) << 8) |
                       (eq_nibble(q0.w, rep) << 12) | (eq_nibble(q1.x, rep) << 16) | (eq_nibble(q1.y, rep) << 20) |
                       (eq_nibble(q1.z, rep) << 24) | (eq_nibble(q1.w, rep) << 28);
@@ -2875,7 +2911,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       } else if (fits && !failed && warp_stage) {
         if (len_ok) {
         bool pieces_done = false;
-        if constexpr (MODE == kModeMulti) {
+        if constexpr (kFreeLike) {
           // Few matches in the region: its output is literal runs between replacements. Each
           // run is copied by the whole warp (aligned 16-byte stores, like a copy-only region),
           // each replacement by as many lanes as it has bytes; no staging of the whole output.
@@ -2886,7 +2922,8 @@ __global__ void __launch_bounds__(kThreads, 3)
             uint32_t i = 0;
             for (uint64_t km = kept; km; km &= km - 1ull, ++i) {
               const uint32_t b = (uint32_t)(__ffsll((long long)km) - 1);
-              const int k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
+              int k = 0;  // the match's pair (kModeMulti)
+              if constexpr (MODE == kModeMulti) k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
               desc[2 * (mb + i)] = lane * 64u + b;  // start within the region
               desc[2 * (mb + i) + 1] = (uint32_t)(k < 0 ? 0 : k);
             }
@@ -2899,14 +2936,14 @@ __global__ void __launch_bounds__(kThreads, 3)
               uint32_t st0 = x0r;
               if (lane > 0) {
                 const uint32_t pk = desc[2 * (lane - 1) + 1];
-                st0 = desc[2 * (lane - 1)] + MT.L[pk];
+                st0 = desc[2 * (lane - 1)] + (MODE == kModeMulti ? (uint32_t)MT.L[pk] : L);
               }
               const uint32_t en = lane < M ? desc[2 * lane] : vend;
               lstart = st0;
               llen = en > st0 ? en - st0 : 0u;
               if (lane < M) {
                 pid = desc[2 * lane + 1];
-                rlen = MT.R[pid];
+                rlen = MODE == kModeMulti ? (uint32_t)MT.R[pid] : R;
               }
             }
             const uint32_t piece = llen + rlen;
@@ -2924,7 +2961,8 @@ __global__ void __launch_bounds__(kThreads, 3)
               if (jp < M) {
                 const uint32_t rl = __shfl_sync(0xffffffffu, rlen, jp);
                 const uint32_t pk = __shfl_sync(0xffffffffu, pid, jp);
-                for (uint32_t q = lane; q < rl; q += 32u) p.out[g0 + po + ll + q] = MT.rep[pk][q];
+                const uint8_t* rb = MODE == kModeMulti ? MT.rep[pk] : rs;  // rs: the replacement (and more)
+                for (uint32_t q = lane; q < rl; q += 32u) p.out[g0 + po + ll + q] = rb[q];
               }
             }
             __syncwarp();
