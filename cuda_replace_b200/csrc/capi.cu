@@ -108,6 +108,7 @@ bool stages_enabled() {
 }
 
 // ------------------------------------------------------------------ page-locked host pool
+using crb::CopyOut;
 using crb::PinnedPool;
 PinnedPool& pinned_pool() { return crb::host_pinned_pool(); }
 
@@ -167,6 +168,7 @@ struct Session {
   // unified() on a large page-locked input: upload and download streams, one event per chunk
   cudaStream_t up = nullptr, down = nullptr;
   cudaEvent_t ev_up[kUnifiedChunks] = {}, ev_done[kUnifiedChunks] = {};
+  cudaEvent_t ev_dl[kUnifiedChunks] = {};   // a chunk's download is done (unified into caller memory)
   cudaEvent_t ev_stage[3] = {};             // a pageable input's staging slots (chunked unified)
   unsigned int* carry2 = nullptr;           // device: carry into / out of the current chunk
   unsigned long long* olen_dev = nullptr;   // device: output end of the current chunk
@@ -294,6 +296,7 @@ void session_free(Session* s) {
   for (int k = 0; k < kUnifiedChunks; ++k) {
     if (s->ev_up[k]) cudaEventDestroy(s->ev_up[k]);
     if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
+    if (s->ev_dl[k]) cudaEventDestroy(s->ev_dl[k]);
   }
   if (s->up) {
     cudaStreamSynchronize(s->up);
@@ -1100,10 +1103,14 @@ CR_EXPORT void cuda_replace_close(void* h) {
 // chunk's upload is queued at once; each chunk is replaced as soon as it is on the device (its
 // last L - 1 bytes held back for the next chunk, the coverage carried across on the device)
 // into the session's output buffer, and its output is downloaded into the result while the
-// next chunks upload. Returns kFallback when the call does not qualify (the caller takes the
-// single-launch path), else 0 or an error code (a cudaError_t, or 999).
+// next chunks upload. With dst (pageable caller memory of at least the worst-case output
+// length), each chunk's output is also copied from that page-locked block into dst by a
+// CopyOut thread as soon as its download lands, while later chunks upload, replace and
+// download; the block goes back to the pool. Returns kFallback when
+// the call does not qualify (the caller takes the single-launch path), else 0 or an error code
+// (a cudaError_t, or 999).
 int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat, uint32_t L, const uint8_t* rep,
-                    uint32_t R, uint8_t** out_host, size_t* out_len) {
+                    uint32_t R, uint8_t** out_host, size_t* out_len, uint8_t* dst = nullptr, size_t dst_cap = 0) {
   if (n < kUnifiedChunkedMin || L == 0 || L > (uint32_t)crb::kInlineMax || R > (uint32_t)crb::kInlineMax)
     return kFallback;
   const bool pinned = host_is_pinned(src);
@@ -1115,6 +1122,7 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   if (!proto.nsub) return kFallback;
   const size_t bound = output_bound(n, L, R);
   if (bound > 4 * n + ((size_t)64 << 20)) return kFallback;  // a large expansion: the single-launch path sizes it
+  if (dst && dst_cap < bound) return kFallback;  // the single-launch path checks the exact length
   memcpy(proto.pat, pat, L);
   if (R) memcpy(proto.rep, rep, R);
   const size_t P = L - 1;  // bytes held back at the end of every chunk but the last
@@ -1133,6 +1141,7 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   for (int k = 0; k < kUnifiedChunks && e == cudaSuccess; ++k) {
     if (!s->ev_up[k]) e = cudaEventCreateWithFlags(&s->ev_up[k], cudaEventDisableTiming);
     if (e == cudaSuccess && !s->ev_done[k]) e = cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming);
+    if (e == cudaSuccess && dst && !s->ev_dl[k]) e = cudaEventCreateWithFlags(&s->ev_dl[k], cudaEventDisableTiming);
   }
   if (e == cudaSuccess && !s->carry2) e = cudaMalloc(&s->carry2, 2 * sizeof(unsigned int));
   if (e == cudaSuccess && !s->olen_dev) e = cudaMalloc(&s->olen_dev, sizeof(unsigned long long));
@@ -1146,6 +1155,8 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
     cudaGetLastError();  // a page-locked block of the worst case was refused: the single-launch
     return kFallback;            // path allocates the result at its exact size
   }
+  CopyOut copyout;
+  if (dst) copyout.open(s->device);
   // Uploads. A page-locked input: every chunk's copy is queued at once. A pageable one: a
   // producer thread copies each chunk (on the copy workers) into one of kStageSlots page-locked
   // staging buffers and queues its upload from there, while this thread replaces and downloads
@@ -1248,6 +1259,10 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
       e = cudaEventRecord(s->ev_done[k], s->stream);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(s->down, s->ev_done[k], 0);
       if (e == cudaSuccess) e = cudaMemcpyAsync(host + O, s->alt + O, olen, cudaMemcpyDeviceToHost, s->down);
+      if (e == cudaSuccess && dst) {
+        e = cudaEventRecord(s->ev_dl[k], s->down);
+        if (e == cudaSuccess) copyout.push(dst + O, host + O, olen, s->ev_dl[k]);
+      }
       if (e != cudaSuccess) {
         rc = (int)e;
         break;
@@ -1257,6 +1272,8 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   }
   stop.store(true);
   if (producer.joinable()) producer.join();
+  const cudaError_t e0 = dst ? copyout.finish() : cudaSuccess;
+  if (rc == 0 && e0 != cudaSuccess) rc = (int)e0;
   const cudaError_t e1 = cudaStreamSynchronize(s->down);
   const cudaError_t e2 = cudaStreamSynchronize(s->up);
   if (rc == 0 && e1 != cudaSuccess) rc = (int)e1;
@@ -1266,6 +1283,11 @@ int unified_chunked(Session* s, const uint8_t* src, size_t n, const uint8_t* pat
   s->len = 0;  // the session's buffers hold no complete content now
   ++s->buf_version;
   s->q_kind = 0;
+  if (dst) {
+    pinned_pool().put(host);  // its downloads and copies are done (both waited for above)
+    if (rc == 0) *out_len = O;
+    return rc;
+  }
   if (rc != 0 || O == 0) {
     pinned_pool().put(host);
     return rc;
@@ -1311,6 +1333,85 @@ CR_EXPORT int cuda_replace_unified(const uint8_t* src, size_t src_len, const uin
   } else {
     session_free(s);
     *out_host = nullptr;
+    *out_len = 0;
+  }
+  return rc;
+}
+
+CR_EXPORT int cuda_replace_output_bound(size_t src_len, int pat_len, int rep_len, size_t* bound) {
+  if (!bound || pat_len < 0 || rep_len < 0) return -1;
+  *bound = output_bound(src_len, (uint32_t)pat_len, (uint32_t)rep_len);
+  return 0;
+}
+
+CR_EXPORT int cuda_replace_unified_into(const uint8_t* src, size_t src_len, const uint8_t* pat, int pat_len,
+                                        const uint8_t* rep, int rep_len, uint8_t* dst, size_t dst_cap,
+                                        size_t* out_len) {
+  if (!out_len || pat_len < 0 || rep_len < 0 || (!src && src_len) || (!pat && pat_len) || (!rep && rep_len))
+    return -1;
+  *out_len = 0;
+  if (pat_len > crb::kInlineMax || rep_len > crb::kInlineMax) return -4;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  Session* s = cache_take(dev);
+  int rc = 0;
+  if (!s) {
+    rc = session_create(&s);
+    if (rc != 0) return rc;
+  }
+  if (pat_len > 0 && dst) {
+    uint8_t* unused = nullptr;
+    rc = unified_chunked(s, src, src_len, pat, (uint32_t)pat_len, rep, (uint32_t)rep_len, &unused, out_len, dst,
+                         dst_cap);
+    if (rc != kFallback) {
+      if (rc == 0) {
+        cache_give(s);
+      } else {
+        session_free(s);
+        *out_len = 0;
+      }
+      return rc;
+    }
+    rc = 0;
+  }
+  rc = session_load(s, src, src_len);
+  if (rc == 0) rc = apply_one(s, pat, pat_len, rep, rep_len, 0, nullptr, nullptr);
+  bool too_small = false;
+  if (rc == 0) {
+    *out_len = s->len;
+    if (s->len > dst_cap) {
+      too_small = true;
+      rc = (int)cudaErrorInvalidValue;  // *out_len tells the length needed
+    } else if (s->len >= ((size_t)32 << 20)) {
+      // downloaded in up to kUnifiedChunks pieces into a pooled page-locked block, each piece
+      // copied into dst as soon as it lands while the next ones download
+      uint8_t* host = static_cast<uint8_t*>(pinned_pool().get(s->len, &e));
+      const size_t piece = round_up((s->len + kUnifiedChunks - 1) / kUnifiedChunks, (size_t)1 << 20);
+      CopyOut copyout;
+      if (host) copyout.open(s->device);
+      for (size_t off = 0, k = 0; host && e == cudaSuccess && off < s->len; off += piece, ++k) {
+        const size_t m = std::min(piece, s->len - off);
+        if (!s->ev_dl[k]) e = cudaEventCreateWithFlags(&s->ev_dl[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host + off, s->buf + off, m, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(s->ev_dl[k], s->stream);
+        if (e == cudaSuccess) copyout.push(dst + off, host + off, m, s->ev_dl[k]);
+      }
+      const cudaError_t e0 = copyout.finish();
+      const cudaError_t e1 = cudaStreamSynchronize(s->stream);
+      if (e == cudaSuccess) e = e0 != cudaSuccess ? e0 : e1;
+      if (host) pinned_pool().put(host);
+      rc = (int)e;
+    } else if (s->len) {
+      e = cudaMemcpyAsync(dst, s->buf, s->len, cudaMemcpyDeviceToHost, s->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+      rc = (int)e;
+    }
+  }
+  if (rc == 0 || too_small) {
+    cache_give(s);
+  } else {
+    session_free(s);
     *out_len = 0;
   }
   return rc;

@@ -166,6 +166,66 @@ class CopyWorkers {
 // memcpy split over the copy workers when it is large.
 inline void parallel_memcpy(void* dst, const void* src, size_t n) { CopyWorkers::get().copy(dst, src, n); }
 
+// Copies ranges of page-locked host memory into pageable caller memory as their downloads
+// land: push() queues (dst, src, n) behind an event recorded after the range's device-to-host
+// copy; a thread of its own waits for each event in turn and copies the range on the copy
+// workers, so the copy of one chunk's output overlaps the downloads and kernels of the next.
+// The downloads themselves go at the link's rate into a page-locked block (a DMA into pageable
+// memory is staged by the driver at a fraction of it). finish() waits for every queued range.
+class CopyOut {
+ public:
+  void open(int device) {
+    th_ = std::thread([this, device] { loop(device); });
+  }
+  void push(uint8_t* dst, const uint8_t* src, size_t n, cudaEvent_t ready) {
+    if (!n) return;
+    std::lock_guard<std::mutex> g(mu_);
+    q_.push_back(Item{dst, src, n, ready});
+    cv_.notify_all();
+  }
+  // waits for every queued range; the first error met (later ranges are skipped after one)
+  cudaError_t finish() {
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      closed_ = true;
+      cv_.notify_all();
+    }
+    if (th_.joinable()) th_.join();
+    return err_;
+  }
+  ~CopyOut() { finish(); }
+
+ private:
+  struct Item {
+    uint8_t* dst;
+    const uint8_t* src;
+    size_t n;
+    cudaEvent_t ready;
+  };
+  void loop(int device) {
+    if (cudaSetDevice(device) != cudaSuccess) err_ = cudaErrorInvalidDevice;
+    for (;;) {
+      Item it;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !q_.empty() || closed_; });
+        if (q_.empty()) break;
+        it = q_.front();
+        q_.erase(q_.begin());
+      }
+      if (err_ != cudaSuccess) continue;
+      if (it.ready) err_ = cudaEventSynchronize(it.ready);
+      if (err_ == cudaSuccess) parallel_memcpy(it.dst, it.src, it.n);
+    }
+  }
+  std::thread th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::vector<Item> q_;
+  bool closed_ = false;
+  cudaError_t err_ = cudaSuccess;  // written by the thread only until finish() joins it
+};
+
 // First-fit sub-allocator over one page-locked block: a server's host staging area, pinned
 // once instead of per request. Blocks handed to callers are released with cuda_free_host
 // (host_free below finds the owning area); an area closed by its server is freed when its

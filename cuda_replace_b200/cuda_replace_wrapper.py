@@ -38,6 +38,43 @@ _bytes_buffer = C.pythonapi.PyBytes_AsString
 _bytes_buffer.restype = C.c_void_p
 _bytes_buffer.argtypes = [C.py_object]
 _PARALLEL_COPY_MIN = 4 << 20
+# The same calls with raw object pointers (new function objects: pythonapi caches the ones
+# above by attribute), for a bytes object filled and shrunk before Python code sees it.
+_new_bytes_raw = C.pythonapi["PyBytes_FromStringAndSize"]
+_new_bytes_raw.restype = C.c_void_p
+_new_bytes_raw.argtypes = [C.c_void_p, C.c_ssize_t]
+_raw_buffer = C.pythonapi["PyBytes_AsString"]
+_raw_buffer.restype = C.c_void_p
+_raw_buffer.argtypes = [C.c_void_p]
+_raw_resize = C.pythonapi["_PyBytes_Resize"]
+_raw_resize.restype = C.c_int
+_raw_resize.argtypes = [C.POINTER(C.c_void_p), C.c_ssize_t]
+_raw_decref = C.pythonapi["Py_DecRef"]
+_raw_decref.restype = None
+_raw_decref.argtypes = [C.c_void_p]
+
+
+def _bytes_filled(n: int, fill) -> bytes:
+    """A bytes object of at most n bytes written by fill(address, n) -> length: created
+    uninitialised at n bytes, filled in place (no second copy of the result), then shrunk to
+    the length written (a realloc that large blocks do in place). The object is private to this
+    function until it returns, so resizing it is allowed (_PyBytes_Resize needs one reference)."""
+    raw = _new_bytes_raw(None, n)
+    if not raw:
+        raise MemoryError(f"bytes object of {n} bytes")
+    try:
+        addr = _raw_buffer(raw)
+        _advise_huge(addr, n)
+        m = fill(addr, n)
+    except BaseException:
+        _raw_decref(raw)
+        raise
+    box = c_void_p(raw)
+    if m != n:
+        _raw_resize(C.byref(box), m)  # raises MemoryError (object freed) if it fails
+    out = C.cast(box, C.py_object).value  # a new reference ...
+    _raw_decref(box)                      # ... and the creation's released
+    return out
 
 
 def _bytes_at(ptr, n: int, lib: Optional[C.CDLL] = None) -> bytes:
@@ -187,6 +224,10 @@ class CudaReplaceLib:
         _bind(lib, "cuda_replace_plan_stages",
               [c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, C.c_int, c_int_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_host_copy", [c_void_p, c_void_p, c_size_t], None, optional=True)
+        _bind(lib, "cuda_replace_unified_into",
+              [c_uint8_p, c_size_t, c_uint8_p, C.c_int, c_uint8_p, C.c_int, c_void_p, c_size_t, c_size_t_p], C.c_int,
+              optional=True)
+        _bind(lib, "cuda_replace_output_bound", [c_size_t, C.c_int, C.c_int, c_size_t_p], C.c_int, optional=True)
         _bind(lib, "cuda_replace_stream",
               [c_uint8_p, c_size_t, c_uint8_pp, c_int_p, c_uint8_pp, c_int_p, C.c_int, c_size_t,
                C.POINTER(c_uint8_p), c_size_t_p], C.c_int, optional=True)
@@ -195,10 +236,29 @@ class CudaReplaceLib:
         return self.lib.cuda_replace_version().decode()
 
     def unified(self, src: bytes, pat: bytes, rep: bytes) -> bytes:
-        """One-shot replace (reference: py:124-141)."""
+        """One-shot replace (reference: py:124-141). A large result is written straight into the
+        returned bytes object (cuda_replace_unified_into): its copy out of page-locked memory
+        overlaps the transfers instead of following them."""
         keep, src_p, n = _src_pointer(src)
         pat_buf = C.create_string_buffer(pat, len(pat) or 1)
         rep_buf = C.create_string_buffer(rep, len(rep) or 1)
+        into = getattr(self.lib, "cuda_replace_unified_into", None)
+        if into is not None and pat and n >= _PARALLEL_COPY_MIN:
+            bound = c_size_t()
+            self.lib.cuda_replace_output_bound(c_size_t(n), C.c_int(len(pat)), C.c_int(len(rep)), C.byref(bound))
+            if bound.value <= 4 * n + (64 << 20):
+                def fill(addr, cap):
+                    got = c_size_t()
+                    rc = into(src_p, c_size_t(n), C.cast(pat_buf, c_uint8_p), C.c_int(len(pat)),
+                              C.cast(rep_buf, c_uint8_p), C.c_int(len(rep)), c_void_p(addr), c_size_t(cap),
+                              C.byref(got))
+                    if rc != 0:
+                        raise RuntimeError(f"cuda_replace_unified_into failed rc={rc}")
+                    return got.value
+                try:
+                    return _bytes_filled(bound.value, fill)
+                finally:
+                    del keep
         out_ptr = c_uint8_p()
         out_len = c_size_t()
         rc = self.lib.cuda_replace_unified(

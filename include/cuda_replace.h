@@ -58,6 +58,27 @@ int cuda_replace_unified(const uint8_t* src, size_t src_len,
                          const uint8_t* rep, int rep_len,
                          uint8_t** out_host, size_t* out_len);
 
+/* cuda_replace_unified into caller memory dst[0, dst_cap) (pageable or page-locked): *out_len
+ * receives the result length. With dst_cap at least cuda_replace_output_bound's worst case, a
+ * src of 256 MiB or more is replaced chunk by chunk; each chunk's output is downloaded into a
+ * pooled page-locked block and copied into dst on the host copy threads as soon as it lands,
+ * while later chunks upload, replace and download (a result of 32 MiB or more from the
+ * single-launch path is downloaded and copied the same way in pieces), so the copy into dst
+ * overlaps the transfers. Returns cudaErrorInvalidValue (1) when dst_cap is below the
+ * result length (*out_len then holds that length; dst is unspecified); -1 for NULL arguments
+ * or negative lengths, -4 for a pattern or replacement above CUDA_REPLACE_MAX_PATTERN.
+ * An addition to the reference's API (its wrapper returns bytes built from the unified result,
+ * cuda_replace_wrapper.py:124-141; this call lets a binding fill its bytes object directly). */
+int cuda_replace_unified_into(const uint8_t* src, size_t src_len,
+                              const uint8_t* pat, int pat_len,
+                              const uint8_t* rep, int rep_len,
+                              uint8_t* dst, size_t dst_cap, size_t* out_len);
+
+/* Worst-case output length of one replace of pat_len bytes by rep_len bytes over src_len bytes
+ * (src_len when rep_len <= pat_len; saturates at SIZE_MAX). -1 for a NULL bound or a negative
+ * length. */
+int cuda_replace_output_bound(size_t src_len, int pat_len, int rep_len, size_t* bound);
+
 /* Release a buffer returned through *out_host.
  * Replaces cuda_free_host (cuda_replace.cu:2559); bound at cuda_replace_wrapper.py:57-58. */
 void cuda_free_host(void* p);

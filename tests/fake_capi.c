@@ -198,3 +198,30 @@ FAKE_EXPORT int cuda_replace_unified(const uint8_t* src, size_t n, const uint8_t
   cuda_replace_close(h);
   return rc;
 }
+
+FAKE_EXPORT int cuda_replace_output_bound(size_t n, int pat_len, int rep_len, size_t* bound) {
+  if (!bound || pat_len < 0 || rep_len < 0) return -1;
+  if (pat_len == 0)
+    *bound = n * ((size_t)rep_len + 1) + (size_t)rep_len;
+  else
+    *bound = rep_len <= pat_len ? n : n + n / (size_t)pat_len * (size_t)(rep_len - pat_len);
+  return 0;
+}
+
+FAKE_EXPORT int cuda_replace_unified_into(const uint8_t* src, size_t n, const uint8_t* pat, int pat_len,
+                                          const uint8_t* rep, int rep_len, uint8_t* dst, size_t cap,
+                                          size_t* out_len) {
+  if (!out_len) return -1;
+  uint8_t* out = NULL;
+  size_t m = 0;
+  const int rc = cuda_replace_unified(src, n, pat, pat_len, rep, rep_len, &out, &m);
+  if (rc) return rc;
+  *out_len = m;
+  if (m > cap) {
+    free(out);
+    return 1; /* cudaErrorInvalidValue: *out_len holds the length needed */
+  }
+  if (m) memcpy(dst, out, m);
+  free(out);
+  return 0;
+}

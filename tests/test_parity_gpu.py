@@ -206,6 +206,61 @@ def test_unified_page_locked_large_chunked(cr_lib):
         del h
 
 
+def test_unified_into_caller_buffer(cr_lib):
+    """cuda_replace_unified_into writes the result into caller memory: the chunked path (input
+    of 256 MiB or more, output downloaded in 32 MiB pieces through page-locked slots and copied
+    out meanwhile) and the single-launch one (smaller inputs; results above and below one piece)
+    equal bytes.replace, also for matches across the chunk joins; a buffer below the result
+    length returns 1 with the length needed; CudaReplaceLib.unified takes this path for large
+    inputs and returns exact bytes objects."""
+    import ctypes as C
+
+    U8P = C.POINTER(C.c_uint8)
+    n = (300 << 20) + 777
+    chunk = max(32 << 20, ((n + 15) // 16 + (1 << 20) - 1) >> 20 << 20)
+    rng = random.Random(43)
+    text = bytearray(rng.randbytes(1 << 20) * (n // (1 << 20) + 1))[:n]
+    for j in range(chunk, n - chunk // 2, chunk):
+        text[j - 3:j + 1] = b"abab"  # straddles the join by one byte
+        text[j + 100:j + 104] = b"abab"
+    text = bytes(text)
+    run = b"a" * n
+
+    def call(src, pat, rep, cap):
+        dst = C.create_string_buffer(max(cap, 1))
+        got = C.c_size_t()
+        pb, rb = C.create_string_buffer(pat, len(pat)), C.create_string_buffer(rep, len(rep) or 1)
+        rc = cr_lib.lib.cuda_replace_unified_into(C.cast(C.c_char_p(src), U8P), len(src), C.cast(pb, U8P), len(pat),
+                                                   C.cast(rb, U8P), len(rep), dst, cap, C.byref(got))
+        return rc, got.value, dst
+
+    def bound(n_, pat, rep):
+        b = C.c_size_t()
+        assert cr_lib.lib.cuda_replace_output_bound(n_, len(pat), len(rep), C.byref(b)) == 0
+        return b.value
+
+    for src, pat, rep in ((text, b"abab", b"X"), (text, b"\x00", b""), (run, b"a", b"bcd"), (run, b"aa", b"X")):
+        want = src.replace(pat, rep)
+        rc, m, dst = call(src, pat, rep, bound(len(src), pat, rep))
+        assert rc == 0 and m == len(want), (pat, rep, rc, m)
+        assert C.string_at(dst, m) == want, (pat, rep)
+        del dst
+        assert cr_lib.unified(src, pat, rep) == want, (pat, rep)
+    # single-launch path: a result above one 32 MiB piece, one below it, and an empty one
+    for size, pat, rep in ((80 << 20, b"a", b"bc"), (5 << 20, b"aa", b"X"), (6 << 20, b"a", b"")):
+        src = b"a" * size
+        want = src.replace(pat, rep)
+        rc, m, dst = call(src, pat, rep, bound(size, pat, rep))
+        assert rc == 0 and m == len(want) and C.string_at(dst, m) == want, (size, pat, rep)
+        assert cr_lib.unified(src, pat, rep) == want
+    # too small a buffer: 1 and the length needed, on both paths
+    for src in (run, b"a" * (8 << 20)):
+        rc, m, _ = call(src, b"a", b"bcd", len(src))
+        assert rc == 1 and m == 3 * len(src)
+    # after the refusals, the cached session still works
+    assert cr_lib.unified(b"xaay" * (2 << 20), b"aa", b"Q") == b"xQy" * (2 << 20)
+
+
 def test_fuzz_runs_blocks_and_text(cr_lib):
     """Seeded inputs of 1-3 MB mixing runs of one byte (often whole 2 KiB regions), short-alphabet
     text and random bytes, against bordered and free patterns of 1-6 bytes and replacements of

@@ -26,6 +26,22 @@ def test_unified_and_session_roundtrip(fake):
         assert s.query_prefix(4) == (2, 3)
 
 
+def test_unified_large_fills_exact_bytes(fake):
+    """unified() on inputs from 4 MiB writes into a bytes object of the worst-case length and
+    shrinks it to the result: shrinking, expanding and unchanged lengths, and an expansion
+    beyond the worst-case rule (taken by the page-locked result path instead)."""
+    import sys
+
+    src = (b"xaay" * (1 << 20)) + b"aa"
+    for pat, rep in ((b"aa", b"Q"), (b"a", b"bcd"), (b"zz", b"Q"), (b"y", b"")):
+        got = fake.unified(src, pat, rep)
+        assert type(got) is bytes and got == src.replace(pat, rep), (pat, rep)
+        assert sys.getrefcount(got) == 2  # the variable and the call's argument: nothing leaked
+        assert hash(got) == hash(bytes(got))
+    big = fake.unified(src, b"x", b"0123456789")  # worst case 10 n: above 4 n + 64 MiB at 16 MiB
+    assert big == src.replace(b"x", b"0123456789")
+
+
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(FileNotFoundError):
         Wr.CudaReplaceLib(str(tmp_path / "nope.so"))
