@@ -1200,7 +1200,7 @@ __device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t 
       return mask;
     }
   }
-  if (L >= 2u && ((p4 >> 8) & 0xFFu) != b0) {
+  if (L >= 3u || (L == 2u && ((p4 >> 8) & 0xFFu) != b0)) {
     // Positions of the first byte, kept in a transposed order that costs fewer operations:
     // bit 8j + i of t0 (t1) is byte j of rotated word i (i + 8). ~((((w ^ rep) & 0x7f..) +
     // 0x7f..) | (w ^ rep)) has bit 7 of a byte set exactly when the byte equals b0; a shift
@@ -2406,7 +2406,8 @@ __global__ void __launch_bounds__(kThreads, 3)
             // (kModeMulti: the replacements differ, so no region is a run of one replacement)
             const bool full = MODE != kModeMulti && 2048u - wcov - wc * L + over == 0u;
             ok = __all_sync(0xffffffffu, !act || full);
-            tin = __all_sync(0xffffffffu, !act || full || wc == 0u);
+            // (kModeFree: a region with at most 16 matches is written as pieces in mode 2)
+            tin = __all_sync(0xffffffffu, !act || full || wc == 0u || (MODE == kModeFree && wc <= 16u));
           }
         }
 #pragma unroll
@@ -2506,6 +2507,68 @@ __global__ void __launch_bounds__(kThreads, 3)
     claim_next();
     if (s_noin[cset] != 1u) ring.push(tcur, 1);
     ring.issue(p, smem, lay, s_bar, S, n16, want_a, n, nsub);
+  };
+
+  // Output of one warp region with at most 16 matches (kFreeLike): literal runs between its
+  // replacements. Each run is copied by the whole warp (aligned 16-byte stores, like a
+  // copy-only region), each replacement by as many lanes as it has bytes; no staging of the
+  // whole output. kept: this thread's kept starts in its 64-byte segment of the sub-tile at tb
+  // (global position gseg); x0r: bytes at the region start covered by an earlier match; vend:
+  // input bytes of the region; the output is out[g0, g0 + wtot). Returns false, writing
+  // nothing, when the region has more than 16 matches; when the pieces do not add up to wtot
+  // (which the arithmetic rules out) it writes nothing and reports an error.
+  auto emit_pieces = [&](const uint8_t* tb, uint64_t kept, unsigned long long gseg, uint32_t x0r, uint32_t vend,
+                         unsigned long long g0, uint32_t wtot) -> bool {
+    const uint32_t cnt = (uint32_t)__popcll(kept);
+    const uint32_t M = __reduce_add_sync(0xffffffffu, cnt);
+    if (M > 16u) return false;
+    uint32_t* desc = reinterpret_cast<uint32_t*>(ob) + (size_t)warp * lay.wstage_words;
+    const uint32_t mb = warp_incl_scan(cnt, OpSum()) - cnt;  // this lane's first match index
+    uint32_t i = 0;
+    for (uint64_t km = kept; km; km &= km - 1ull, ++i) {
+      const uint32_t b = (uint32_t)(__ffsll((long long)km) - 1);
+      int k = 0;  // the match's pair (kModeMulti)
+      if constexpr (MODE == kModeMulti) k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
+      desc[2 * (mb + i)] = lane * 64u + b;  // start within the region
+      desc[2 * (mb + i) + 1] = (uint32_t)(k < 0 ? 0 : k);
+    }
+    __syncwarp();
+    // piece j (lane j <= M): the literal run before match j (after the last match for j = M)
+    uint32_t lstart = 0, llen = 0, rlen = 0, pid = 0;
+    if (lane <= M) {
+      uint32_t st0 = x0r;
+      if (lane > 0) {
+        const uint32_t pk = desc[2 * (lane - 1) + 1];
+        st0 = desc[2 * (lane - 1)] + (MODE == kModeMulti ? (uint32_t)MT.L[pk] : L);
+      }
+      const uint32_t en = lane < M ? desc[2 * lane] : vend;
+      lstart = st0;
+      llen = en > st0 ? en - st0 : 0u;
+      if (lane < M) {
+        pid = desc[2 * lane + 1];
+        rlen = MODE == kModeMulti ? (uint32_t)MT.R[pid] : R;
+      }
+    }
+    const uint32_t piece = llen + rlen;
+    const uint32_t poff = warp_incl_scan(piece, OpSum()) - piece;
+    // the pieces fill exactly the region's slot (the same sum as the threads' lengths);
+    // otherwise nothing is written and the launch reports an error
+    const bool pieces_ok = __shfl_sync(0xffffffffu, poff + piece, 31) == wtot;
+    if (!pieces_ok && lane == 0) set_error(p);
+    for (uint32_t jp = 0; pieces_ok && jp <= M; ++jp) {
+      const uint32_t ls = __shfl_sync(0xffffffffu, lstart, jp);
+      const uint32_t ll = __shfl_sync(0xffffffffu, llen, jp);
+      const uint32_t po = __shfl_sync(0xffffffffu, poff, jp);
+      if (ll) warp_emit_literal(p.out, tb, g0 + po, ll, warp * 2048u + ls);
+      if (jp < M) {
+        const uint32_t rl = __shfl_sync(0xffffffffu, rlen, jp);
+        const uint32_t pk = __shfl_sync(0xffffffffu, pid, jp);
+        const uint8_t* rb = MODE == kModeMulti ? MT.rep[pk] : rs;  // rs: the replacement (and more)
+        for (uint32_t q = lane; q < rl; q += 32u) p.out[g0 + po + ll + q] = rb[q];
+      }
+    }
+    __syncwarp();
+    return true;
   };
 
   // look-back, pass B and records of super-tile t, whose pass A filled set `set`; after the
@@ -2663,9 +2726,15 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
       const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
       const uint32_t offr = incl - olen_r;
-      noin_last1 = __reduce_max_sync(0xffffffffu, wc ? jr * (uint32_t)kTile + wr * 2048u + x0 + (wc - 1u) * L + 1u : 0u);
-      // a region not shown by the fold: literal bytes beside kept matches
-      const bool odd = __any_sync(0xffffffffu, olen_r != wc * R && wc != 0u);
+      // the last kept start: kModeFree, the region's last match ends at its cover end `we`
+      // (from the sub-tile start); otherwise the region is a run x0, x0 + L, ...
+      noin_last1 = __reduce_max_sync(
+          0xffffffffu, wc ? (MODE == kModeFree ? jr * (uint32_t)kTile + we - L + 1u
+                                               : jr * (uint32_t)kTile + wr * 2048u + x0 + (wc - 1u) * L + 1u)
+                          : 0u);
+      // a region not shown by the fold: literal bytes beside kept matches (kModeFree: beside
+      // more than 16 of them; fewer are written as pieces)
+      const bool odd = __any_sync(0xffffffffu, olen_r != wc * R && wc > (MODE == kModeFree ? 16u : 0u));
       const bool fits_t = (O + total <= p.out_cap) && (O <= p.out_cap);
       if (!fits_t && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
       if (odd && tid == 0) set_error(p);
@@ -2678,11 +2747,16 @@ __global__ void __launch_bounds__(kThreads, 3)
         const uint32_t cr = __shfl_sync(0xffffffffu, wc, r);
         const uint32_t xr = __shfl_sync(0xffffffffu, x0, r);
         if (write && ol) {
-          if (cr == 0u)
+          if (cr == 0u) {
             warp_emit_literal(p.out, tb, O + of, ol, warp * 2048u + xr);
-          else
+          } else if (ol == cr * R) {
             warp_emit_replace(p.out, reinterpret_cast<const uint4*>(smem + lay.tab16), rs, R, step512, rmag,
                               O + of, ol);
+          } else if constexpr (MODE == kModeFree) {
+            // matches beside literal bytes (at most 16, as the fold checked; all kept in free mode)
+            emit_pieces(tb, masks_s[j * kThreads + tid], tstart + (unsigned long long)j * kTile + sb, xr, 2048u,
+                        O + of, ol);
+          }
         }
         __syncthreads();
         ring.release();
@@ -2912,62 +2986,9 @@ __global__ void __launch_bounds__(kThreads, 3)
         if (len_ok) {
         bool pieces_done = false;
         if constexpr (kFreeLike) {
-          // Few matches in the region: its output is literal runs between replacements. Each
-          // run is copied by the whole warp (aligned 16-byte stores, like a copy-only region),
-          // each replacement by as many lanes as it has bytes; no staging of the whole output.
-          const uint32_t M = __reduce_add_sync(0xffffffffu, cnt);
-          if (M <= 16u) {
-            uint32_t* desc = reinterpret_cast<uint32_t*>(ob) + (size_t)warp * lay.wstage_words;
-            const uint32_t mb = warp_incl_scan(cnt, OpSum()) - cnt;  // this lane's first match index
-            uint32_t i = 0;
-            for (uint64_t km = kept; km; km &= km - 1ull, ++i) {
-              const uint32_t b = (uint32_t)(__ffsll((long long)km) - 1);
-              int k = 0;  // the match's pair (kModeMulti)
-              if constexpr (MODE == kModeMulti) k = multi_identify(MT, tb + sb + b, n_all - (gseg + b));
-              desc[2 * (mb + i)] = lane * 64u + b;  // start within the region
-              desc[2 * (mb + i) + 1] = (uint32_t)(k < 0 ? 0 : k);
-            }
-            __syncwarp();
-            const uint32_t x0r = __shfl_sync(0xffffffffu, x_in, 0);  // covered at the region start
-            const uint32_t vend = __reduce_add_sync(0xffffffffu, V);  // input bytes of the region
-            // piece j (lane j <= M): the literal run before match j (after the last match for j = M)
-            uint32_t lstart = 0, llen = 0, rlen = 0, pid = 0;
-            if (lane <= M) {
-              uint32_t st0 = x0r;
-              if (lane > 0) {
-                const uint32_t pk = desc[2 * (lane - 1) + 1];
-                st0 = desc[2 * (lane - 1)] + (MODE == kModeMulti ? (uint32_t)MT.L[pk] : L);
-              }
-              const uint32_t en = lane < M ? desc[2 * lane] : vend;
-              lstart = st0;
-              llen = en > st0 ? en - st0 : 0u;
-              if (lane < M) {
-                pid = desc[2 * lane + 1];
-                rlen = MODE == kModeMulti ? (uint32_t)MT.R[pid] : R;
-              }
-            }
-            const uint32_t piece = llen + rlen;
-            const uint32_t poff = warp_incl_scan(piece, OpSum()) - piece;
-            const unsigned long long g0 = O + wbase;
-            // the pieces fill exactly the region's slot (the same sum as the threads' lengths);
-            // otherwise nothing is written and the launch reports an error
-            const bool pieces_ok = __shfl_sync(0xffffffffu, poff + piece, 31) == wtot;
-            if (!pieces_ok && lane == 0) set_error(p);
-            for (uint32_t jp = 0; pieces_ok && jp <= M; ++jp) {
-              const uint32_t ls = __shfl_sync(0xffffffffu, lstart, jp);
-              const uint32_t ll = __shfl_sync(0xffffffffu, llen, jp);
-              const uint32_t po = __shfl_sync(0xffffffffu, poff, jp);
-              if (ll) warp_emit_literal(p.out, tb, g0 + po, ll, warp * 2048u + ls);
-              if (jp < M) {
-                const uint32_t rl = __shfl_sync(0xffffffffu, rlen, jp);
-                const uint32_t pk = __shfl_sync(0xffffffffu, pid, jp);
-                const uint8_t* rb = MODE == kModeMulti ? MT.rep[pk] : rs;  // rs: the replacement (and more)
-                for (uint32_t q = lane; q < rl; q += 32u) p.out[g0 + po + ll + q] = rb[q];
-              }
-            }
-            __syncwarp();
-            pieces_done = true;
-          }
+          // few matches in the region: literal runs between replacements
+          pieces_done = emit_pieces(tb, kept, gseg, __shfl_sync(0xffffffffu, x_in, 0),
+                                    __reduce_add_sync(0xffffffffu, V), O + wbase, wtot);
         }
         if (!pieces_done) {
         uint32_t W[17];
