@@ -1639,41 +1639,111 @@ __device__ __forceinline__ void fn_scan_down(uint32_t g[4], uint32_t step) {
   if ((threadIdx.x & 31u) + step < 32u) fn_after<LL>(g, o);
 }
 
-// Look-back for patterns of LL <= 4 bytes over the 16-byte records. Each window of 32
-// predecessors is composed by a scan over lanes (lane l: super-tile t - 1 - l, the identity at
-// and beyond the nearest inclusive one), so a window costs a few shuffle steps whatever its
-// length.
+
+// Window of 64 predecessors, two per lane: lane l reads super-tiles base - 2l and base - 2l - 1
+// (distances 2l and 2l + 1; distance < 0: the virtual inclusive tile before tile 0). Returns the
+// distance of the nearest inclusive record (64 if none) once every nearer record is valid, or
+// -1 when the wait gave up; d0/d1 receive the payloads. Both loads of a lane are in flight
+// together, so a window costs one round trip.
+__device__ __forceinline__ int warp_read_window2(const ReplaceParams& p, long long base, unsigned long long d0[2],
+                                                 unsigned long long d1[2], uint32_t carry0) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t tag = p.epoch & 0xFFFFFFu;
+  unsigned long long t0 = 0;
+  uint32_t ns = 32;
+  for (;;) {
+    uint32_t st[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const long long j = base - 2 * (long long)lane - r;
+      st[r] = 0;
+      d0[r] = 0;
+      d1[r] = 0;
+      if (j < 0) {
+        st[r] = kStInc;
+        d1[r] = carry0;  // the virtual tile before tile 0 leaves carry0 bytes covered
+      } else {
+        rec_load(p.rec, (uint32_t)j, &d0[r], &d1[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      if (base - 2 * (long long)lane - r >= 0) {
+        const unsigned long long w0 = d0[r], w1 = d1[r];
+        const uint32_t s0 = (uint32_t)(w0 >> 38) & 3u, s1 = (uint32_t)(w1 >> 38) & 3u;
+        st[r] = ((uint32_t)(w0 >> 40) == tag && (uint32_t)(w1 >> 40) == tag && s0 == s1) ? s0 : 0u;
+        d0[r] = rec_data(w0);
+        d1[r] = rec_data(w1);
+      }
+    }
+    // this lane's nearest inclusive record (2: none) and whether every nearer one is valid
+    const uint32_t fi = st[0] == kStInc ? 0u : (st[1] == kStInc ? 1u : 2u);
+    const bool pre = (fi < 1u || st[0] != 0u) && (fi < 2u || st[1] != 0u);
+    const uint32_t incm = __ballot_sync(0xffffffffu, fi < 2u);
+    const uint32_t okm = __ballot_sync(0xffffffffu, pre);
+    const uint32_t pl = incm ? (uint32_t)(__ffs(incm) - 1) : 32u;
+    const uint32_t need = pl >= 31u ? 0xffffffffu : ((2u << pl) - 1u);  // lanes 0..pl
+    if ((okm & need) == need) {
+      const uint32_t fpl = __shfl_sync(0xffffffffu, fi, pl & 31u);
+      return pl == 32u ? 64 : (int)(2u * pl + fpl);
+    }
+    if (aborted(p)) return -1;
+    const unsigned long long now = global_ns();
+    if (t0 == 0) {
+      t0 = now;
+    } else if (now - t0 > kSpinLimitNs) {
+      if (lane == 0) set_error(p);
+      return -1;
+    }
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+  }
+}
+
+// Look-back for patterns of LL <= 4 bytes over the 16-byte records, in windows of 64
+// predecessors (warp_read_window2): each lane first composes its two super-tiles' functions
+// (the older applied first), then a scan over lanes (lane l: super-tiles t - 1 - 2l and
+// t - 2 - 2l, the identity at and beyond the nearest inclusive one) composes the window, so a
+// window costs a few shuffle steps whatever its length. Counts stay within 24 bits: 64
+// super-tiles of at most 2^15 kept starts.
 template <int LL>
 __device__ __forceinline__ bool lookback_small_rec(const ReplaceParams& p, uint32_t t, unsigned long long* K_out,
-                                                   uint32_t* c_out, uint32_t carry0) {
+                                                    uint32_t* c_out, uint32_t carry0) {
   const uint32_t lane = threadIdx.x & 31u;
   unsigned long long acc_cnt = 0;  // lane c < LL: function of the super-tiles between the window and t
   uint32_t acc_carry = lane;
   long long base = (long long)t - 1;
   for (;;) {
-    unsigned long long d0, d1;
-    const int plr = warp_read_window(p, base, &d0, &d1, carry0);
-    if (plr < 0) return false;
-    const uint32_t pl = (uint32_t)plr;
-    uint32_t g[4];
+    unsigned long long d0[2], d1[2];
+    const int D = warp_read_window2(p, base, d0, d1, carry0);
+    if (D < 0) return false;
+    uint32_t g[4], f[4];
 #pragma unroll
     for (uint32_t y = 0; y < (uint32_t)LL; ++y) {
       g[y] = y << 24;
-      if (lane < pl) {
-        const uint32_t e = tab4_entry(d0, d1, y);
+      f[y] = y << 24;
+      if (2u * lane + 1u < (uint32_t)D) {  // the older record of the lane
+        const uint32_t e = tab4_entry(d0[1], d1[1], y);
         g[y] = (e & 0x1FFFFu) | ((e >> 17) << 24);
       }
+      if (2u * lane < (uint32_t)D) {  // the nearer one
+        const uint32_t e = tab4_entry(d0[0], d1[0], y);
+        f[y] = (e & 0x1FFFFu) | ((e >> 17) << 24);
+      }
     }
-    fn_scan_down<LL>(g, 1);
-    fn_scan_down<LL>(g, 2);
-    fn_scan_down<LL>(g, 4);
-    fn_scan_down<LL>(g, 8);
-    fn_scan_down<LL>(g, 16);
+    fn_after<LL>(f, g);  // the nearer applied after the older
+    fn_scan_down<LL>(f, 1);
+    fn_scan_down<LL>(f, 2);
+    fn_scan_down<LL>(f, 4);
+    fn_scan_down<LL>(f, 8);
+    fn_scan_down<LL>(f, 16);
     // lane 0 now holds the window's function (its oldest super-tile applied first)
-    if (pl < 32) {
-      const unsigned long long K = __shfl_sync(0xffffffffu, d0, pl);  // the inclusive one
-      const uint32_t x = (uint32_t)__shfl_sync(0xffffffffu, d1, pl);
-      const uint32_t e = __shfl_sync(0xffffffffu, fn_at<LL>(g, x), 0);
+    if (D < 64) {
+      const uint32_t ln = (uint32_t)D >> 1;
+      const bool older = (D & 1) != 0;
+      const unsigned long long K = __shfl_sync(0xffffffffu, older ? d0[1] : d0[0], ln);  // the inclusive one
+      const uint32_t x = (uint32_t)__shfl_sync(0xffffffffu, older ? d1[1] : d1[0], ln);
+      const uint32_t e = __shfl_sync(0xffffffffu, fn_at<LL>(f, x), 0);
       const uint32_t xc = e >> 24;
       *K_out = K + (e & 0xFFFFFFu) + __shfl_sync(0xffffffffu, acc_cnt, xc);
       *c_out = __shfl_sync(0xffffffffu, acc_carry, xc);
@@ -1681,14 +1751,14 @@ __device__ __forceinline__ bool lookback_small_rec(const ReplaceParams& p, uint3
     }
     uint32_t w[4];
 #pragma unroll
-    for (uint32_t y = 0; y < (uint32_t)LL; ++y) w[y] = __shfl_sync(0xffffffffu, g[y], 0);
+    for (uint32_t y = 0; y < (uint32_t)LL; ++y) w[y] = __shfl_sync(0xffffffffu, f[y], 0);
     const uint32_t e = fn_at<LL>(w, lane < (uint32_t)LL ? lane : 0u);  // entry `lane` of the window
     const uint32_t y = e >> 24;
     const unsigned long long ac = __shfl_sync(0xffffffffu, acc_cnt, y);
     const uint32_t ax = __shfl_sync(0xffffffffu, acc_carry, y);
     acc_cnt = (e & 0xFFFFFFu) + ac;
     acc_carry = ax;
-    base -= 32;
+    base -= 64;
   }
 }
 
