@@ -261,6 +261,43 @@ def test_unified_into_caller_buffer(cr_lib):
     assert cr_lib.unified(b"xaay" * (2 << 20), b"aa", b"Q") == b"xQy" * (2 << 20)
 
 
+def test_pieces_threshold_in_regions(cr_lib):
+    """Free-mode super-tiles whose 2 KiB warp regions hold 0-64 matches: regions with at most 16
+    are written as literal runs between replacements (table-driven pass B), a super-tile with a
+    region above 16 takes the general pass B. Matches at region starts and ends, straddling
+    region and super-tile edges, back to back, shrinking, deleting and expanding: bytes.replace
+    exactly, through Session.apply (one launch) and unified."""
+    rng = random.Random(47)
+    pat = b"&te;"
+    region, super_tile = 2048, 4 * TILE
+    n = 96 * super_tile + 777
+    buf = bytearray(rng.choice(b"abcdefgh ;") for _ in range(n))
+    counts = [0, 1, 2, 3, 15, 16, 17, 31, 32, 64]
+    for r in range(n // region - 1):
+        k = counts[r % len(counts)] if (r // 32) % 3 else counts[(r * 7) % 6]  # some super-tiles stay <= 16
+        base = r * region
+        if k == 0:
+            continue
+        if r % 5 == 0:  # back to back from the region start
+            pos = [base + 4 * i for i in range(k)]
+        else:
+            pos = sorted(rng.sample(range(base, base + region - 4, 4), k))
+        for q in pos:
+            buf[q:q + 4] = pat
+    for e in range(super_tile, n - 8, super_tile):  # straddling super-tile edges
+        off = rng.randrange(1, 4)
+        buf[e - off:e - off + 4] = pat
+    for e in range(region * 3, n - 8, region * 11):  # straddling region edges
+        buf[e - 2:e + 2] = pat
+    src = bytes(buf)
+    for rep in (b"6n", b"", b"XYZ12345", b"&"):
+        want = src.replace(pat, rep)
+        with Wr.Session(cr_lib, src) as s:
+            assert s.apply(pat, rep) == len(want)
+            assert s.result() == want, rep
+        assert cr_lib.unified(src, pat, rep) == want, rep
+
+
 def test_fuzz_runs_blocks_and_text(cr_lib):
     """Seeded inputs of 1-3 MB mixing runs of one byte (often whole 2 KiB regions), short-alphabet
     text and random bytes, against bordered and free patterns of 1-6 bytes and replacements of
