@@ -2054,6 +2054,22 @@ struct LoadRing {
   __device__ __forceinline__ void release() { ++consumed; }
 };
 
+// k output chunks of one lane of warp_emit_literal, 512 bytes apart (the warp's 32 lanes
+// interleaved): the word offset Q of the source within its 16-byte chunk is the same for every
+// chunk of a call, so the loop is instantiated per offset (no selection inside it) and kept
+// rolled (unrolled copies of the four instances spilled registers).
+template <int Q>
+__device__ __forceinline__ void literal_chunks(uint8_t* dst, const uint8_t* src, uint32_t k, uint32_t sh) {
+#pragma unroll 1
+  for (; k; --k) {
+    const uint4 A = *reinterpret_cast<const uint4*>(src);
+    const uint4 B = *reinterpret_cast<const uint4*>(src + 16u);
+    st_out16(dst, extract16(A, B, (uint32_t)Q, sh));
+    src += 512u;
+    dst += 512u;
+  }
+}
+
 // One warp's output when it is a copy of its input: wtot bytes from tile byte srcw, written at
 // out[g0, g0 + wtot) with aligned 16-byte stores (funnel-shifted from shared memory); the
 // partial 16-byte chunks at both ends one byte per lane (the neighbouring regions own their
@@ -2067,11 +2083,19 @@ __device__ __forceinline__ void warp_emit_literal(uint8_t* out, const uint8_t* t
   const uint32_t c1 = (uint32_t)((gend - ga) >> 4);        // end of the whole chunks
   const uint32_t off0 = srcw + (uint32_t)(ga + ((unsigned long long)c0 << 4) - g0);
   const uint32_t r = off0 & 15u, q = r >> 2, sh = (r & 3u) * 8u;
-  for (uint32_t c = c0 + lane; c < c1; c += 32u) {
-    const uint32_t a = off0 - r + ((c - c0) << 4);
-    const uint4 A = *reinterpret_cast<const uint4*>(tb + a);
-    const uint4 B = *reinterpret_cast<const uint4*>(tb + a + 16u);
-    st_out16(out + ga + ((unsigned long long)c << 4), extract16(A, B, q, sh));
+  {
+    const uint32_t c = c0 + lane;
+    if (c < c1) {
+      const uint32_t k = (c1 - c + 31u) >> 5;  // this lane's chunks c, c + 32, ...
+      const uint8_t* src = tb + (off0 - r + ((c - c0) << 4));
+      uint8_t* dst = out + ga + ((unsigned long long)c << 4);
+      switch (q) {  // the same in every lane
+        case 0: literal_chunks<0>(dst, src, k, sh); break;
+        case 1: literal_chunks<1>(dst, src, k, sh); break;
+        case 2: literal_chunks<2>(dst, src, k, sh); break;
+        default: literal_chunks<3>(dst, src, k, sh); break;
+      }
+    }
   }
   unsigned long long b;
   bool ok;
