@@ -2341,6 +2341,9 @@ __global__ void __launch_bounds__(kThreads, 3)
     const unsigned long long lim =
         MODE == kModeMulti ? n : ((n_all >= L) ? min(n_all - L + 1, n) : 0ull);  // candidates p < lim
     const bool edge = tstart < p.block_before || tstart + (unsigned long long)m * kTile > lim;
+    // (this and the other per-sub-tile loops are kept rolled: their bodies are large, and
+    // unrolled copies measured about 1% slower)
+#pragma unroll 1
     for (uint32_t j = 0; j < m; ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long gseg = tstart + (unsigned long long)j * kTile + sb;
@@ -2469,6 +2472,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         uint32_t cnt_sum = 0;
         int dsum = 0;      // kModeMulti: sum of R - L over the super-tile's matches
         long long lco_max = LLONG_MIN;
+#pragma unroll 1
         for (uint32_t j0 = 0; j0 < m; j0 += 4u) {
           const uint32_t jr = j0 + (lane >> 3);
           const bool act = jr < m;
@@ -2532,6 +2536,7 @@ __global__ void __launch_bounds__(kThreads, 3)
         else
           fold_small_rec<4>(wt, s_dense[set], wrec_b, subrec_b, m, whole, &bad, &mixed, &sup_cnt, &sup_carry);
       } else
+#pragma unroll 1
       for (uint32_t j = 0; j < m; ++j) {
         uint8_t* wrec = wrec_b + (size_t)j * kWarps * L;
         uint32_t y = lane < L ? lane : 0u, cnt = 0;
@@ -2838,6 +2843,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       if (!fits_t && tid == 0) atomicExch(&p.res->overflow_epoch, p.epoch);
       if (odd && tid == 0) set_error(p);
       const bool write = fits_t && !odd && !failed;
+#pragma unroll 1
       for (uint32_t j = 0; j < m; ++j) {
         const uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
         const uint32_t r = j * kWarps + warp;
@@ -2867,6 +2873,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     // ================= pass B: exact kept starts and output, one warp region at a time
     uint32_t csub = cin;      // kModeFree: carry into sub-tile j
     long long last_abs = -1;  // last kept start seen by this thread
+#pragma unroll 1
     for (uint32_t j = 0; j < (pbm != 0u ? 0u : m); ++j) {
       uint8_t* tb = ring.wait(p, smem, lay, s_bar, &s_fail);
       const unsigned long long sstart = tstart + (unsigned long long)j * kTile;
