@@ -1223,16 +1223,17 @@ __device__ __forceinline__ uint64_t candidates_seg(const uint8_t* seg, uint32_t 
       return candidates_from_words(w, p4, m4);
     }
     uint64_t out = 0;
-    for (int h = 0; h < 2; ++h) {
-      uint32_t m = h ? t1 : t0;
-      while (m) {
-        const uint32_t b = (uint32_t)(__ffs(m) - 1);
-        m &= m - 1u;
-        const uint32_t i = (b & 7u) + 8u * (uint32_t)h;                    // rotated word
-        const uint32_t nat = (((rot + (i >> 2)) & 3u) << 2) | (i & 3u);  // natural word
-        const uint32_t pos = 4u * nat + (b >> 3);
-        if (((ld_u32_unaligned(seg + pos) ^ p4) & m4) == 0u) out |= 1ull << pos;
-      }
+    // one loop over both halves (t0's positions, then t1's): a warp iterates as often as its
+    // busiest lane has positions in all
+    while (t0 | t1) {
+      const uint32_t h = t0 ? 0u : 1u;
+      const uint32_t m = h ? t1 : t0;
+      const uint32_t b = (uint32_t)(__ffs(m) - 1);
+      if (h) t1 = m & (m - 1u); else t0 = m & (m - 1u);
+      const uint32_t i = (b & 7u) + 8u * h;                              // rotated word
+      const uint32_t nat = (((rot + (i >> 2)) & 3u) << 2) | (i & 3u);  // natural word
+      const uint32_t pos = 4u * nat + (b >> 3);
+      if (((ld_u32_unaligned(seg + pos) ^ p4) & m4) == 0u) out |= 1ull << pos;
     }
     return out;
   }
