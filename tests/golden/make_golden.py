@@ -97,7 +97,7 @@ def defect_vectors():
         case("empty input", [], [(b"a", b"b")], "edge"),
         case("pattern longer than input", [[h(b"ab"), 1]], [(b"abc", b"X")], "edge"),
         case("embedded NULs deletion", [[h(b"\x00\x00\x01\x00\x00\x00\x01\x01"), 3]],
-             [(b"\x00\x00\x01", b"")], "BASELINE config 2 (iii) shape"),
+             [(b"\x00\x00\x01", b"")], "single-pair workload shape: random 00 00 01 deleted"),
     ]
 
 
@@ -145,7 +145,7 @@ def config_digests():
     gens.append({"fn": "text_corpus", "n": 2 * MiB, "seed": 3, "name": "C3 scaled 2 MiB text x 128 pairs"})
     rows = []
     for g in gens:
-        row = {"name": g.pop("name"), "source": "BASELINE configs (scaled)", "generator": g}
+        row = {"name": g.pop("name"), "source": "stated workload configurations (scaled)", "generator": g}
         src, pairs = config_inputs(row)
         out = O.chain(src, pairs)
         row.update({"in_len": len(src), "in_sha256": sha(src), "npairs": len(pairs),
